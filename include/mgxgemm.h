@@ -1,0 +1,214 @@
+/*
+ * mgxgemm.h -- C ABI of libmgxgemm, the B200 (sm_100a) per-rank FP64 block-multiply path of
+ * MGXBench.
+ *
+ * MGXBench's GPU work is three host functions in mulmat_kernel.cu, declared by its drivers at
+ * 1D-row-block/mmb.cu:162-164 and 2D-block-matrix/mmb.cu:20-22:
+ *     void ABMultiply(double*, double*, double*, int m, int n, int k, int lda, int ldb, int ldc, int w);
+ *     void ABMultiplyAccumulateAsync(const double*, const double*, double*, int m, int n, int k_total,
+ *                                    int k_offset, int k_chunk, int lda, int ldb, int ldc, int w,
+ *                                    cudaStream_t);
+ *     int  validate_matrix_C(const double*, int rows, int cols, double expected, double abs_tol,
+ *                            double rel_tol, int rank);
+ * The mgx_ab_* / mgx_validate_* entry points below replace them one for one, with the same
+ * argument meaning (row-major matrices, leading dimensions in elements, device pointers owned
+ * by the caller).  Where the reference aborts or ignores errors, these return a status code.
+ *
+ * Conventions
+ *   - Every pointer argument named a, b, c, A, B, C is a device pointer.
+ *   - Matrices are row-major: element (i, j) of X is X[i * ldx + j].
+ *   - Functions taking a `stream` (a cudaStream_t passed as void*, NULL = legacy default stream)
+ *     are stream-ordered and return after launching.  The others synchronise.
+ *   - Return value: MGX_SUCCESS (0) or a negative mgx_status_t; mgx_last_error_message() says more.
+ *   - No function exits or aborts the process.
+ *   - Thread safety: calls on different host threads are safe; device work that overlaps on the
+ *     GPU shares nothing unless a comment says otherwise.
+ */
+#ifndef MGXGEMM_H
+#define MGXGEMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MGX_API __attribute__((visibility("default")))
+#else
+#define MGX_API
+#endif
+
+typedef enum {
+    MGX_SUCCESS = 0,
+    MGX_E_INVALID = -1,      /* an argument is out of range (sizes, leading dimensions, null pointer) */
+    MGX_E_CUDA = -2,         /* a CUDA runtime or driver call failed */
+    MGX_E_NONFINITE = -3,    /* the Ozaki form met a NaN or infinity in A or B */
+    MGX_E_TIMEOUT = -4,      /* a bounded device-side wait ran out (kernel abandoned its work) */
+    MGX_E_WORKSPACE = -5,    /* workspace pointer null or smaller than required */
+    MGX_E_UNSUPPORTED = -6,  /* no kernel for this device / configuration */
+    MGX_E_DEVICE = -7        /* the kernel reported another device-side error */
+} mgx_status_t;
+
+/* Result of a constant-value validation (validate_C_kernel semantics). */
+typedef struct {
+    uint64_t elements;       /* rows * cols */
+    uint64_t invalid;        /* elements with abs err > abs_tol AND rel err > rel_tol, or non-finite */
+    double max_abs_error;
+    double max_rel_error;
+} mgx_validation_t;
+
+/* Error of a computed C against a double-double reference product of the same A and B. */
+typedef struct {
+    double normwise;         /* ||C - AB||_F / ||AB||_F */
+    double max_rel;          /* max |C - AB| / |AB| over elements with |AB| >= floor_rel * max|AB| */
+    double max_componentwise;/* max |C - AB| / (|A||B|) */
+    double max_abs;          /* max |C - AB| */
+    uint64_t rows_checked;
+} mgx_error_t;
+
+/* ------------------------------------------------------------------------------------------
+ * Drop-in replacements for MGXBench's launchers
+ * ------------------------------------------------------------------------------------------ */
+
+/* Replaces ABMultiply (1D-row-block/mulmat_kernel.cu:86-92; 2D-block-matrix/mulmat_kernel.cu:81-87):
+ * C[m x n] = A[m x k] * B[k x n] on the legacy default stream, asynchronously.  `w` is the
+ * reference's tile width (TILE_DIM = 32); it must be positive and does not change the result or
+ * the tiling this library uses. */
+MGX_API int mgx_ab_multiply(double *a, double *b, double *c, int m, int n, int k, int lda, int ldb, int ldc,
+                            int w);
+
+/* Replaces ABMultiplyAccumulateAsync (1D-row-block/mulmat_kernel.cu:148-158;
+ * 2D-block-matrix/mulmat_kernel.cu:142-151):
+ * C[m x n] += A[:, k_offset : k_offset + k_chunk] * B_chunk[k_chunk x n], the chunk's product
+ * summed first and then added to C with one rounding, as the reference does.  Columns of A at
+ * or beyond k_total read as zero. */
+MGX_API int mgx_ab_multiply_accumulate_async(const double *a, const double *b_chunk, double *c, int m, int n,
+                                             int k_total, int k_offset, int k_chunk, int lda, int ldb, int ldc,
+                                             int w, void *stream);
+
+/* Replaces validate_matrix_C (1D-row-block/mulmat_kernel.cu:228-326; 2D copy :221-304):
+ * checks every element of the rows x cols device matrix against `expected`, prints the
+ * reference's NUMERICAL VALIDATION block on stdout when rank == 0 and print != 0, fills *out
+ * when out != NULL, and returns 1 (pass), 0 (fail) or a negative mgx_status_t.  Unlike the
+ * reference it also counts NaN and infinite elements as invalid. Synchronous. */
+MGX_API int mgx_validate_matrix_c(const double *d_c, int rows, int cols, double expected, double abs_tol,
+                                  double rel_tol, int rank, int print, mgx_validation_t *out);
+
+/* ------------------------------------------------------------------------------------------
+ * Native FP64 GEMM (FP64 tensor-core MMA, TMA-fed warp-specialised pipeline)
+ * ------------------------------------------------------------------------------------------ */
+
+/* C = A B (beta_one == 0) or C += A B (beta_one != 0), A m x k, B k x n, all FP64. */
+MGX_API int mgx_gemm_fp64(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                          int ldc, int beta_one, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Ozaki-scheme FP64 GEMM on the INT8 tensor cores (tcgen05, exact int32 TMEM accumulation)
+ * ------------------------------------------------------------------------------------------ */
+
+/* Bytes of device workspace mgx_gemm_ozaki needs for this shape and split count. */
+MGX_API size_t mgx_ozaki_workspace_size(int m, int n, int k, int splits);
+
+/* C = A B or C += A B computed as the exact integer products of `splits` signed 7-bit digit
+ * slices per operand (per-row / per-column power-of-two scaling), recombined in FP64.
+ * splits in [2, 12].  Returns MGX_E_NONFINITE if A or B holds NaN or infinity. */
+MGX_API int mgx_gemm_ozaki(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                           int ldc, int beta_one, int splits, void *workspace, size_t workspace_bytes,
+                           void *stream);
+
+/* The two phases of mgx_gemm_ozaki for one K range of at most mgx_ozaki_kmax(splits):
+ * mgx_ozaki_split writes the exponents and digit slices of A and B into the workspace;
+ * mgx_ozaki_multiply runs the INT8 tensor-core products and the FP64 recombination into C.
+ * Calling split once and multiply several times reuses the slices. */
+MGX_API int mgx_ozaki_split(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int splits,
+                            void *workspace, size_t workspace_bytes, void *stream);
+MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ldc, int beta_one, int splits,
+                               const void *workspace, size_t workspace_bytes, void *stream);
+
+/* Largest K one int32 accumulation of `splits`-digit slices can take (mgx_gemm_ozaki splits K
+ * into chunks of this size and adds them in order). */
+MGX_API int mgx_ozaki_kmax(int splits);
+
+/* Split count the library picks to reach a normwise relative error <= target for inputs whose
+ * per-row / per-column dynamic range is `exp_range` binades (a-priori model; 3..9). */
+MGX_API int mgx_ozaki_choose_splits(int k, double exp_range, double target);
+
+/* ------------------------------------------------------------------------------------------
+ * 2D SUMMA over a process grid, all blocks and panels on this GPU
+ *
+ * Replaces the panel loop of 2D-block-matrix/mmb.cu:239-361 for every rank of a grid_rows x
+ * grid_cols process grid at once: block (i, j) owns rows [row_cuts[i], row_cuts[i+1]) and
+ * columns [col_cuts[j], col_cuts[j+1]) of C, and C = 0 followed by C_ij += A_i[:, k0:k0+kc]
+ * B_j[k0:k0+kc, :] for every panel of width panel_k.  The plan runs all (block, tile, panel)
+ * work in ONE persistent kernel launch (plus the split kernels of the Ozaki form), so a run can
+ * be captured in a CUDA graph.  Blocks need not be equal (uneven splits, remainders).
+ * ------------------------------------------------------------------------------------------ */
+
+typedef enum { MGX_FORM_FP64 = 0, MGX_FORM_OZAKI = 1 } mgx_form_t;
+
+typedef struct {
+    int m, n, k;               /* C is m x n, the reduction is k */
+    int grid_rows, grid_cols;  /* Pr x Pc process grid (2D-block-matrix/mmb.cu:45-58) */
+    const int *row_cuts;       /* grid_rows + 1 ascending row boundaries; NULL = split evenly, the
+                                  first (m mod Pr) blocks one row taller */
+    const int *col_cuts;       /* likewise for columns */
+    int panel_k;               /* panel width BK (MGXBENCH_SUMMA_BK, 2D-block-matrix/mmb.cu:107) */
+    int form;                  /* mgx_form_t */
+    int splits;                /* slices of the Ozaki form */
+} mgx_summa_desc_t;
+
+typedef struct mgx_summa_plan mgx_summa_plan_t;
+
+/* Builds the work list on the current device and allocates the Ozaki workspace if needed. */
+MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t **plan);
+
+/* C = SUMMA product of A (m x k, lda) and B (k x n, ldb); stream-ordered, allocates nothing. */
+MGX_API int mgx_summa_run(mgx_summa_plan_t *plan, const double *A, int lda, const double *B, int ldb, double *C,
+                          int ldc, void *stream);
+
+/* Work tiles (128 x 128, clipped to their blocks), panels and workspace bytes of a plan. */
+MGX_API int mgx_summa_plan_info(const mgx_summa_plan_t *plan, int *work_tiles, int *panels, size_t *workspace_bytes);
+
+MGX_API int mgx_summa_plan_destroy(mgx_summa_plan_t *plan);
+
+/* ------------------------------------------------------------------------------------------
+ * Accuracy checking on the GPU (double-double reference product)
+ * ------------------------------------------------------------------------------------------ */
+
+/* Error of C (m x n) against A B computed in double-double, over `row_count` rows starting at
+ * `row_start` (all rows when row_count <= 0).  Synchronous. */
+MGX_API int mgx_error_vs_dd(const double *A, const double *B, const double *C, int m, int n, int k, int lda,
+                            int ldb, int ldc, int row_start, int row_count, double floor_rel, mgx_error_t *out);
+
+/* ------------------------------------------------------------------------------------------
+ * Synthetic inputs
+ * ------------------------------------------------------------------------------------------ */
+
+/* Fills rows x cols of X (leading dimension ld) on the device: kind 0 = the constant `value`
+ * (MGXBench's A = 1, B = 2 initialisation, 1D-row-block/mmb.cu:586-591), 1 = uniform [-1, 1),
+ * 2 = u * 2^e with u uniform [-1, 1) and e a uniform integer in [-e_range, e_range].  Element
+ * (r, c) depends only on (seed, r * cols + c).  Stream-ordered. */
+MGX_API int mgx_fill_matrix(double *X, int rows, int cols, int ld, int kind, double value, int e_range,
+                            uint64_t seed, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Library state
+ * ------------------------------------------------------------------------------------------ */
+
+/* Reads and clears the current device's status word written by bounded device-side waits
+ * (0 = none).  Synchronises the device. */
+MGX_API int mgx_device_status(int *code_out);
+
+MGX_API const char *mgx_last_error_message(void);
+MGX_API const char *mgx_status_string(int status);
+
+/* Measured peaks of this GPU's FP64 paths: kind 0 = DFMA on the FP64 units, 1 = DMMA m8n8k4,
+ * 2 = DMMA m16n8k4, 3 = DMMA m16n8k8, 4 = DMMA m16n8k16.  Synchronous; writes TFLOP/s. */
+MGX_API int mgx_peak_fp64(int kind, int iterations, double *tflops_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGXGEMM_H */

@@ -1,0 +1,255 @@
+// capi.cu -- extern "C" entry points of libmgxgemm (declared in include/mgxgemm.h) and the host
+// bookkeeping shared by the kernels' translation units.
+#include <cudaTypedefs.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "mgx_common.cuh"
+
+// ------------------------------------------------------------------------------- host state
+namespace {
+thread_local char g_msg[512] = "";
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+int *g_status_ptr[kMaxDevices];       // device address of mgx_status_word, per device
+int g_sm_count[kMaxDevices];
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+}  // namespace
+
+// One status word per device; kernels record the first device-side error here.
+__device__ int mgx_status_word;
+
+void mgx_set_last_message(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_msg, sizeof g_msg, fmt, ap);
+    va_end(ap);
+}
+
+void mgx_set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line)
+{
+    mgx_set_last_message("%s failed at %s:%d: %s", what, file, line, cudaGetErrorString(e));
+}
+
+static int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    return dev;
+}
+
+int *mgx_device_status_ptr()
+{
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_status_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, mgx_status_word) != cudaSuccess) return nullptr;
+        g_status_ptr[dev] = static_cast<int *>(p);
+    }
+    return g_status_ptr[dev];
+}
+
+int mgx_sm_count()
+{
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices) return 148;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_sm_count[dev]) {
+        int c = 0;
+        if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0) c = 148;
+        g_sm_count[dev] = c;
+    }
+    return g_sm_count[dev];
+}
+
+static int get_encoder()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_encode) return MGX_SUCCESS;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+        mgx_set_last_message("cuTensorMapEncodeTiled unavailable (%s)", cudaGetErrorString(e));
+        return MGX_E_UNSUPPORTED;
+    }
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return MGX_SUCCESS;
+}
+
+int mgx_encode_tmap_2d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_bytes, const void *base, uint64_t inner,
+                       uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer,
+                       CUtensorMapSwizzle swizzle)
+{
+    (void)elem_bytes;
+    const int rc = get_encoder();
+    if (rc != MGX_SUCCESS) return rc;
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {row_stride_bytes};
+    cuuint32_t box[2] = {box_inner, box_outer};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(map, dtype, 2, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        mgx_set_last_message("cuTensorMapEncodeTiled(2d) failed with %d", (int)r);
+        return MGX_E_CUDA;
+    }
+    return MGX_SUCCESS;
+}
+
+int mgx_encode_tmap_3d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_bytes, const void *base, uint64_t d0,
+                       uint64_t d1, uint64_t d2, uint64_t stride1_bytes, uint64_t stride2_bytes, uint32_t b0,
+                       uint32_t b1, uint32_t b2, CUtensorMapSwizzle swizzle)
+{
+    (void)elem_bytes;
+    const int rc = get_encoder();
+    if (rc != MGX_SUCCESS) return rc;
+    cuuint64_t dims[3] = {d0, d1, d2};
+    cuuint64_t strides[2] = {stride1_bytes, stride2_bytes};
+    cuuint32_t box[3] = {b0, b1, b2};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = g_encode(map, dtype, 3, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        mgx_set_last_message("cuTensorMapEncodeTiled(3d) failed with %d", (int)r);
+        return MGX_E_CUDA;
+    }
+    return MGX_SUCCESS;
+}
+
+// Defined in the kernels' translation units.
+int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
+                     int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic);
+int mgx_validate_impl(const double *d_c, size_t count, double expected, double abs_tol, double rel_tol,
+                      mgx_validation_t *out, cudaStream_t stream);
+
+static bool dims_ok(int m, int n, int k, int lda, int ldb, int ldc)
+{
+    if (m < 0 || n < 0 || k < 0) return false;
+    if (lda < (k > 0 ? k : 1) && m > 0 && k > 0) return false;
+    if (ldb < (n > 0 ? n : 1) && k > 0 && n > 0) return false;
+    if (ldc < (n > 0 ? n : 1) && m > 0 && n > 0) return false;
+    return true;
+}
+
+extern "C" {
+
+MGX_API const char *mgx_last_error_message(void) { return g_msg; }
+
+MGX_API const char *mgx_status_string(int status)
+{
+    switch (status) {
+    case MGX_SUCCESS: return "success";
+    case MGX_E_INVALID: return "invalid argument";
+    case MGX_E_CUDA: return "CUDA error";
+    case MGX_E_NONFINITE: return "non-finite input";
+    case MGX_E_TIMEOUT: return "device-side wait timed out";
+    case MGX_E_WORKSPACE: return "workspace missing or too small";
+    case MGX_E_UNSUPPORTED: return "unsupported configuration";
+    case MGX_E_DEVICE: return "device-side error";
+    default: return "unknown status";
+    }
+}
+
+MGX_API int mgx_device_status(int *code_out)
+{
+    int *p = mgx_device_status_ptr();
+    if (!p) {
+        mgx_set_last_message("no device status word (no CUDA device?)");
+        return MGX_E_CUDA;
+    }
+    MGX_HOST_CHECK(cudaDeviceSynchronize());
+    int code = 0;
+    MGX_HOST_CHECK(cudaMemcpy(&code, p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (code != 0) {
+        const int zero = 0;
+        MGX_HOST_CHECK(cudaMemcpy(p, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (code_out) *code_out = code;
+    return MGX_SUCCESS;
+}
+
+MGX_API int mgx_gemm_fp64(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                          int ldc, int beta_one, void *stream)
+{
+    if (!dims_ok(m, n, k, lda, ldb, ldc) || (m > 0 && n > 0 && (!C || (k > 0 && (!A || !B))))) {
+        mgx_set_last_message("mgx_gemm_fp64: invalid arguments m=%d n=%d k=%d lda=%d ldb=%d ldc=%d", m, n, k, lda,
+                             ldb, ldc);
+        return MGX_E_INVALID;
+    }
+    return mgx_launch_dgemm(A, B, C, m, n, k, 0, k, k, lda, ldb, ldc, beta_one ? 1 : 0, (cudaStream_t)stream, 0);
+}
+
+MGX_API int mgx_ab_multiply(double *a, double *b, double *c, int m, int n, int k, int lda, int ldb, int ldc, int w)
+{
+    if (w <= 0) {
+        mgx_set_last_message("mgx_ab_multiply: tile width w=%d must be positive", w);
+        return MGX_E_INVALID;
+    }
+    return mgx_gemm_fp64(a, b, c, m, n, k, lda, ldb, ldc, 0, nullptr);
+}
+
+MGX_API int mgx_ab_multiply_accumulate_async(const double *a, const double *b_chunk, double *c, int m, int n,
+                                             int k_total, int k_offset, int k_chunk, int lda, int ldb, int ldc,
+                                             int w, void *stream)
+{
+    if (w <= 0 || m < 0 || n < 0 || k_chunk < 0 || k_offset < 0 || k_total < 0 ||
+        (m > 0 && n > 0 && k_chunk > 0 && (!a || !b_chunk || !c || lda < 1 || ldb < n || ldc < n))) {
+        mgx_set_last_message("mgx_ab_multiply_accumulate_async: invalid arguments");
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0 || k_chunk == 0) return MGX_SUCCESS;
+    int a_x_end = k_offset + k_chunk;
+    if (a_x_end > k_total) a_x_end = k_total;
+    if (a_x_end <= k_offset) {
+        // Every A column of the chunk is outside k_total: the reference multiplies zeros.
+        // Route it through the generic kernel so 0 * B keeps the reference's NaN behaviour.
+        return mgx_launch_dgemm(a, b_chunk, c, m, n, k_chunk, k_offset, k_offset, k_chunk, lda, ldb, ldc, 1,
+                                (cudaStream_t)stream, 1);
+    }
+    return mgx_launch_dgemm(a, b_chunk, c, m, n, k_chunk, k_offset, a_x_end, k_chunk, lda, ldb, ldc, 1,
+                            (cudaStream_t)stream, 0);
+}
+
+MGX_API int mgx_validate_matrix_c(const double *d_c, int rows, int cols, double expected, double abs_tol,
+                                  double rel_tol, int rank, int print, mgx_validation_t *out)
+{
+    if (rows < 0 || cols < 0 || (rows > 0 && cols > 0 && !d_c)) {
+        mgx_set_last_message("mgx_validate_matrix_c: invalid arguments");
+        return MGX_E_INVALID;
+    }
+    mgx_validation_t v;
+    const size_t count = (size_t)rows * (size_t)cols;
+    const int rc = mgx_validate_impl(d_c, count, expected, abs_tol, rel_tol, &v, nullptr);
+    if (rc != MGX_SUCCESS) return rc;
+    if (out) *out = v;
+    if (rank == 0 && print) {
+        // Same block and formats as validate_matrix_C (1D-row-block/mulmat_kernel.cu:298-319).
+        printf("\n");
+        printf("============================================================\n");
+        printf("NUMERICAL VALIDATION\n");
+        printf("============================================================\n");
+        printf("Matrix dimensions  : %d x %d\n", rows, cols);
+        printf("Expected C[i,j]    : %.12f\n", expected);
+        printf("Elements checked   : %llu\n", (unsigned long long)count);
+        printf("Invalid elements   : %llu\n", (unsigned long long)v.invalid);
+        printf("Max absolute error : %.6e\n", v.max_abs_error);
+        printf("Max relative error : %.6e\n", v.max_rel_error);
+        printf("Absolute tolerance : %.6e\n", abs_tol);
+        printf("Relative tolerance : %.6e\n", rel_tol);
+        printf("Result             : %s\n", v.invalid == 0 ? "PASS" : "FAIL");
+        printf("============================================================\n");
+        fflush(stdout);
+    }
+    return v.invalid == 0 ? 1 : 0;
+}
+
+}  // extern "C"

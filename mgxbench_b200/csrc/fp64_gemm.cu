@@ -1,0 +1,386 @@
+// fp64_gemm.cu -- native FP64 GEMM for sm_100a on the FP64 tensor-core path (DMMA).
+//
+// Replaces the arithmetic of MGXBench's sharedABMultiply / sharedABMultiplyAccumulate
+// (1D-row-block/mulmat_kernel.cu:39-80 and 100-142): C = A*B, or C += (A*B summed over the chunk).
+//
+// Design (one CTA per SM, persistent):
+//   * warp 8 (producer): one lane issues TMA 2D tile loads of A (128 x 32 doubles, two 128-byte
+//     swizzled boxes) and B (32 x 128 doubles, eight boxes) into a 3-stage ring, each stage
+//     guarded by a full/empty mbarrier pair.  No multicast.
+//   * warps 0-7 (consumers): a 2 x 4 warp grid, each warp owning a 64 x 32 block of the
+//     128 x 128 output tile as 4 x 4 DMMA m16n8k4 accumulators (64 doubles per lane).
+//   * The reduction index is permuted inside every group of 8 (physical order 0,1,4,5 | 2,3,6,7)
+//     identically for A and B, so each fragment load from the swizzled tiles hits every shared
+//     memory bank exactly twice (the minimum for 256 bytes).
+//   * Epilogue: C = acc (beta 0) or C = C + acc (beta 1), one rounding, as the reference.
+// A variant whose producer warp loads with plain global loads handles layouts TMA cannot
+// describe (odd leading dimensions, misaligned pointers, odd K offsets).
+#include <cstdio>
+
+#include "mgx_common.cuh"
+
+namespace mgx {
+namespace fp64 {
+
+constexpr int BM = 128, BN = 128, BK = 32;
+constexpr int STAGES = 3;
+constexpr int CWARPS = 8;
+constexpr int THREADS = (CWARPS + 1) * 32;
+constexpr int A_BOX_BYTES = 128 * 128;       // 128 rows x 16 doubles
+constexpr int B_BOX_BYTES = BK * 128;        // 32 rows x 16 doubles
+constexpr int A_STAGE_BYTES = 2 * A_BOX_BYTES;
+constexpr int B_STAGE_BYTES = 8 * B_BOX_BYTES;
+constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;  // 64 KiB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int GROUP_M = 8;
+
+struct Params {
+    const double *A;  // generic loader only
+    const double *B;
+    double *C;
+    int m, n;
+    int k_len;        // reduction length handled by this call
+    int a_x0;         // first column of A (k_offset)
+    int a_x_end;      // A columns >= a_x_end read as zero (min(k_total, k_offset + k_chunk))
+    int b_rows;       // rows of B (chunk) that exist; rows >= b_rows read as zero
+    int lda, ldb, ldc;
+    int beta_one;
+    int vec_store;    // C rows 16-byte aligned (ldc even, C aligned)
+    int *status;
+    const int4 *tiles;  // optional work list (m0, n0, m_end, n_end); null -> regular tiling of m x n
+    int num_tiles;
+    int panel_kb;       // > 0: add the accumulator into C after every panel_kb K blocks (SUMMA panels)
+};
+
+__device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn);
+
+__device__ __forceinline__ void tile_bounds(const Params &p, int tile, int tiles_m, int tiles_n, int &m0, int &n0,
+                                            int &m_end, int &n_end)
+{
+    if (p.tiles) {
+        const int4 t = p.tiles[tile];
+        m0 = t.x;
+        n0 = t.y;
+        m_end = t.z;
+        n_end = t.w;
+    } else {
+        int tm, tn;
+        tile_coords(tile, tiles_m, tiles_n, tm, tn);
+        m0 = tm * BM;
+        n0 = tn * BN;
+        m_end = p.m;
+        n_end = p.n;
+    }
+}
+
+__device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn)
+{
+    const int per_group = GROUP_M * tiles_n;
+    const int group = tile / per_group;
+    const int first_m = group * GROUP_M;
+    const int gsize = min(tiles_m - first_m, GROUP_M);
+    const int r = tile % per_group;
+    tm = first_m + r % gsize;
+    tn = r / gsize;
+}
+
+// Swizzled byte offset of element (row, col16) inside a box whose rows are 128 bytes.
+__device__ __forceinline__ uint32_t sw128(int row, int col16)
+{
+    return row * 128 + ((((col16 >> 1) ^ (row & 7)) & 7) << 4) + ((col16 & 1) << 3);
+}
+
+template <bool USE_TMA>
+__global__ void __launch_bounds__(THREADS, 1)
+    dgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                            ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], USE_TMA ? 1 : 32);
+            mbar_init(&empty[s], CWARPS);
+        }
+        fence_barrier_init();
+    }
+    if (USE_TMA && warp == CWARPS && lane == 0) {
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    __syncthreads();
+
+    const int tiles_m = (p.m + BM - 1) / BM;
+    const int tiles_n = (p.n + BN - 1) / BN;
+    const int tiles = p.tiles ? p.num_tiles : tiles_m * tiles_n;
+    const int kblocks = (p.k_len + BK - 1) / BK;
+
+    if (warp == CWARPS) {
+        // ------------------------------------------------------------ producer
+        int stage = 0;
+        uint32_t phase = 0;
+        int armed_parity[STAGES];
+        for (int s = 0; s < STAGES; ++s) armed_parity[s] = -1;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+            int m0, n0, m_end, n_end;
+            tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end);
+            for (int kb = 0; kb < kblocks; ++kb) {
+                bool got = true;
+                if (lane == 0) got = mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty);
+                got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
+                __syncwarp();
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *sA = smem + stage * STAGE_BYTES;
+                unsigned char *sB = sA + A_STAGE_BYTES;
+                const int k0 = kb * BK;
+                if (USE_TMA) {
+                    if (lane == 0) {
+                        mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                        armed_parity[stage] = (int)phase;
+                        tma_load_2d(sA, &tmA, p.a_x0 + k0, m0, &full[stage]);
+                        tma_load_2d(sA + A_BOX_BYTES, &tmA, p.a_x0 + k0 + 16, m0, &full[stage]);
+                        for (int j = 0; j < 8; ++j) tma_load_2d(sB + j * B_BOX_BYTES, &tmB, n0 + 16 * j, k0, &full[stage]);
+                    }
+                } else {
+                    // A tile: 128 rows x 32 columns, one row per warp iteration (coalesced)
+                    for (int r = 0; r < BM; ++r) {
+                        const int row = m0 + r;
+                        const int kk = k0 + lane;
+                        const int acol = p.a_x0 + kk;
+                        double v = 0.0;
+                        if (row < p.m && kk < p.k_len && acol < p.a_x_end) v = p.A[(size_t)row * p.lda + acol];
+                        const int h = lane >> 4;
+                        *reinterpret_cast<double *>(sA + h * A_BOX_BYTES + sw128(r, lane & 15)) = v;
+                    }
+                    // B tile: 32 rows x 128 columns
+                    for (int r = 0; r < BK; ++r) {
+                        const int brow = k0 + r;
+                        for (int c = lane; c < BN; c += 32) {
+                            const int col = n0 + c;
+                            double v = 0.0;
+                            if (brow < p.b_rows && brow < p.k_len && col < p.n) v = p.B[(size_t)brow * p.ldb + col];
+                            *reinterpret_cast<double *>(sB + (c >> 4) * B_BOX_BYTES + sw128(r, c & 15)) = v;
+                        }
+                    }
+                    mbar_arrive(&full[stage]);
+                }
+                if (++stage == STAGES) {
+                    stage = 0;
+                    phase ^= 1u;
+                }
+            }
+        }
+        // Never leave the CTA with a tensor copy still writing its shared memory.
+        if (USE_TMA && lane == 0) {
+            for (int s = 0; s < STAGES; ++s)
+                if (armed_parity[s] >= 0) mbar_wait_bounded(&full[s], (uint32_t)armed_parity[s], p.status, kDevTimeoutFull);
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    const int wm = warp >> 2;  // 0..1
+    const int wn = warp & 3;   // 0..3
+    const int g = lane >> 2;
+    const int t = lane & 3;
+
+    int stage = 0;
+    uint32_t phase = 0;
+    const uint32_t smem_base = smem_u32(smem);
+
+    // Per-lane parts of the fragment addresses (see the header comment for the permutation).
+    uint32_t a_row_off[4][2];
+    for (int mt = 0; mt < 4; ++mt)
+        for (int h = 0; h < 2; ++h) a_row_off[mt][h] = (uint32_t)((wm * 64 + mt * 16 + h * 8 + g) * 128 + ((t & 1) << 3));
+
+    // C (+)= acc for this lane's fragments, masked to the tile's bounds.
+    auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int beta_one) {
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
+                if (row >= m_end) continue;
+                double *crow = p.C + (size_t)row * p.ldc;
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    const int col = n0 + wn * 32 + nt * 8 + 2 * t;
+                    double v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
+                    if (p.vec_store && col + 1 < n_end) {
+                        double2 *dst = reinterpret_cast<double2 *>(crow + col);
+                        if (beta_one) {
+                            const double2 old = *dst;
+                            v0 = old.x + v0;
+                            v1 = old.y + v1;
+                        }
+                        *dst = make_double2(v0, v1);
+                    } else {
+                        if (col < n_end) crow[col] = beta_one ? crow[col] + v0 : v0;
+                        if (col + 1 < n_end) crow[col + 1] = beta_one ? crow[col + 1] + v1 : v1;
+                    }
+                }
+            }
+        }
+    };
+
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        int m0, n0, m_end, n_end;
+        tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end);
+
+        double acc[4][4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+
+        bool ok = true;
+        for (int kb = 0; kb < kblocks; ++kb) {
+            bool got = true;
+            if (lane == 0) got = mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull);
+            got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
+            if (!got) {
+                ok = false;
+                break;
+            }
+            const uint32_t sA = smem_base + stage * STAGE_BYTES;
+            const uint32_t sB = sA + A_STAGE_BYTES;
+#pragma unroll
+            for (int kb8 = 0; kb8 < 4; ++kb8) {
+#pragma unroll
+                for (int step = 0; step < 2; ++step) {
+                    const int phys = (t & 1) + ((t >> 1) << 2) + 2 * step;  // k within the group of 8
+                    const uint32_t a_chunk = (uint32_t)((((kb8 & 1) * 4 + (t >> 1) * 2 + step) ^ g) << 4);
+                    double a0[4], a1[4], b0[4];
+#pragma unroll
+                    for (int mt = 0; mt < 4; ++mt) {
+                        const uint32_t base = sA + (kb8 >> 1) * A_BOX_BYTES + a_chunk;
+                        a0[mt] = lds_f64(base + a_row_off[mt][0]);
+                        a1[mt] = lds_f64(base + a_row_off[mt][1]);
+                    }
+#pragma unroll
+                    for (int nt = 0; nt < 4; ++nt) {
+                        const int j = wn * 2 + (nt >> 1);
+                        const int krow = kb8 * 8 + phys;
+                        const uint32_t off = (uint32_t)(j * B_BOX_BYTES + krow * 128 +
+                                                        (((((nt & 1) * 4) + (g >> 1)) ^ phys) << 4) + ((g & 1) << 3));
+                        b0[nt] = lds_f64(sB + off);
+                    }
+#pragma unroll
+                    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                        for (int nt = 0; nt < 4; ++nt) dmma_16x8x4(acc[mt][nt], a0[mt], a1[mt], b0[nt]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage]);
+            if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1u;
+            }
+            if (p.panel_kb > 0 && ((kb + 1) % p.panel_kb == 0) && kb + 1 < kblocks) {
+                // end of a SUMMA panel: C_ij += panel product, one rounding, as the reference
+                store_acc(acc, m0, n0, m_end, n_end, 1);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+            }
+        }
+        if (!ok) return;
+        store_acc(acc, m0, n0, m_end, n_end, p.panel_kb > 0 ? 1 : p.beta_one);
+    }
+}
+
+}  // namespace fp64
+}  // namespace mgx
+
+using namespace mgx;
+
+static int tiles_list_or(const int4 *tiles, int num_tiles, int m, int n)
+{
+    return tiles ? num_tiles : ((m + fp64::BM - 1) / fp64::BM) * ((n + fp64::BN - 1) / fp64::BN);
+}
+
+// Launch C (+)= A[:, a_x0 : a_x0 + k_len] * B[0 : k_len, :] with the library's FP64 kernel.
+// a_x_end: A columns at or beyond it read as zero; b_rows: rows of B that exist.
+int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
+                        int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
+                        const int4 *tiles, int num_tiles, int panel_kb)
+{
+    if (m <= 0 || n <= 0) return MGX_SUCCESS;
+    if (k_len <= 0) {
+        if (beta_one) return MGX_SUCCESS;
+        // C = A*B with an empty reduction is zero
+        MGX_HOST_CHECK(cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)n * sizeof(double), m, stream));
+        return MGX_SUCCESS;
+    }
+    fp64::Params p;
+    p.A = A;
+    p.B = B;
+    p.C = C;
+    p.m = m;
+    p.n = n;
+    p.k_len = k_len;
+    p.a_x0 = a_x0;
+    p.a_x_end = a_x_end;
+    p.b_rows = b_rows;
+    p.lda = lda;
+    p.ldb = ldb;
+    p.ldc = ldc;
+    p.beta_one = beta_one;
+    p.vec_store = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+    p.status = mgx_device_status_ptr();
+    p.tiles = tiles;
+    p.num_tiles = num_tiles;
+    p.panel_kb = panel_kb;
+
+    const bool tma_ok = !force_generic && ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
+                        ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (lda % 2 == 0) && (ldb % 2 == 0) &&
+                        (a_x0 % 2 == 0) && a_x_end > 0 && b_rows > 0;
+    CUtensorMap tmA, tmB;
+    memset(&tmA, 0, sizeof tmA);
+    memset(&tmB, 0, sizeof tmB);
+    bool use_tma = false;
+    if (tma_ok) {
+        const int ea = mgx_encode_tmap_2d(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, (uint64_t)a_x_end, (uint64_t)m,
+                                          (uint64_t)lda * 8, 16, 128, CU_TENSOR_MAP_SWIZZLE_128B);
+        const int eb = mgx_encode_tmap_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, B, (uint64_t)n, (uint64_t)b_rows,
+                                          (uint64_t)ldb * 8, 16, fp64::BK, CU_TENSOR_MAP_SWIZZLE_128B);
+        use_tma = (ea == MGX_SUCCESS && eb == MGX_SUCCESS);
+    }
+    const int total_tiles = tiles_list_or(tiles, num_tiles, m, n);
+    int grid = mgx_sm_count();
+    if (grid > total_tiles) grid = total_tiles;
+    if (use_tma) {
+        MGX_HOST_CHECK(cudaFuncSetAttribute(fp64::dgemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            fp64::SMEM_BYTES));
+        fp64::dgemm_kernel<true><<<grid, fp64::THREADS, fp64::SMEM_BYTES, stream>>>(tmA, tmB, p);
+    } else {
+        MGX_HOST_CHECK(cudaFuncSetAttribute(fp64::dgemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            fp64::SMEM_BYTES));
+        fp64::dgemm_kernel<false><<<grid, fp64::THREADS, fp64::SMEM_BYTES, stream>>>(tmA, tmB, p);
+    }
+    MGX_HOST_CHECK(cudaGetLastError());
+    return MGX_SUCCESS;
+}
+
+int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
+                     int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic)
+{
+    return mgx_launch_dgemm_ex(A, B, C, m, n, k_len, a_x0, a_x_end, b_rows, lda, ldb, ldc, beta_one, stream,
+                               force_generic, nullptr, 0, 0);
+}

@@ -1,0 +1,780 @@
+// ozaki.cu -- FP64-accurate GEMM on the INT8 tensor cores (Ozaki scheme; Ozaki, Ogita, Oishi &
+// Rump 2012, "Error-free transformations of matrix multiplication by using fast routines of
+// matrix multiplication and its applications"; Ootomo, Ozaki & Yokota 2024, "DGEMM on integer
+// matrix multiplication unit").
+//
+// Algorithm (s = number of slices):
+//   ea_i = e such that max_k |a_ik| in [2^(e-1), 2^e); eb_j likewise for column j of B.
+//   x = a_ik * 2^(6 - ea_i) (|x| < 64); digit_t = rint(x), x <- (x - digit_t) * 128, t = 1..s.
+//   Every digit is an integer in [-64, 64]; a_ik = 2^(ea_i - 6) sum_t digit_t 2^(-7(t-1)) + tail.
+//   G_d = sum_{t+u=d} sum_k DA_t[i,k] DB_u[j,k] for d = 2..s+1 is exact in int32 while
+//   s * 64 * 64 * K < 2^31 (the host splits K beyond that).
+//   h = 0; for d = s+1 down to 2: h = fma(h, 2^-7, G_d);   C_ij (+)= h * 2^(ea_i + eb_j - 12).
+//
+// Kernels:
+//   ozaki_row_exp   row maxima of A (one warp per row)
+//   ozaki_col_max   column maxima of B (atomicMax on the bit pattern of |b|)
+//   ozaki_split_a   digits of A as [t][i][kp] int8 (K-major)
+//   ozaki_split_b   digits of B transposed to [u][j][kp] int8 (K-major) through shared memory
+//   ozaki_gemm      persistent tcgen05 kernel, one 128 x 128 output tile at a time:
+//       warp 0      TMA producer: for each 32-byte K block, the slices a weight set needs
+//                   (128 rows x 32 bytes each, 32-byte swizzle) into a 3-stage ring
+//       warp 1      TMEM owner and MMA issuer: tcgen05.mma.kind::i8, M=128 N=128 K=32, one
+//                   int32 accumulator (128 TMEM columns) per weight group, four groups per set
+//       warps 2-9   epilogue: tcgen05.ld of each group, FP64 Horner update held in registers
+//                   across sets (highest weights first), final power-of-two scaling and store
+// All waits are bounded (mgx_common.cuh); TMEM is always released before the CTA exits.
+#include <cstdio>
+#include <cstring>
+
+#include "mgx_common.cuh"
+
+namespace mgx {
+namespace oz {
+
+constexpr int TILE = 128;              // output tile is TILE x TILE
+constexpr int KBLK = 32;               // bytes of K per stage (one MMA instruction)
+constexpr int SLICE_TILE_BYTES = TILE * KBLK;  // 4 KiB
+constexpr int MAX_SPLITS = 12;
+constexpr int MAX_SETS = 3;            // ceil(12 / 4): up to four weight groups (4 x 128 TMEM columns) per set
+constexpr int EPI_WARPS = 8;
+constexpr int THREADS = (2 + EPI_WARPS) * 32;
+constexpr int NONFINITE_EXP = 0x7fffffff;
+
+struct GemmParams {
+    double *C;
+    int m, n, ldc;
+    int kblocks;              // ceil(kp / 32)
+    int splits;
+    int num_sets;
+    int set_dhi[MAX_SETS];    // highest weight of each set (sets ordered by decreasing weight)
+    int set_dlo[MAX_SETS];
+    int stage_bytes;          // 2 * splits * 4 KiB
+    int stages;
+    const int *ea;            // row exponents of A
+    const int *eb;            // column exponents of B
+    const int4 *tiles;        // optional work list (m0, n0, m_end, n_end); null -> regular tiling
+    int num_tiles;
+    int beta_one;
+    int vec_store;
+    int *status;
+};
+
+// ---------------------------------------------------------------- shared numerics
+__host__ __device__ __forceinline__ int frexp_exp_bits(unsigned long long absbits)
+{
+    if (absbits == 0) return 0;
+    const int biased = (int)(absbits >> 52);
+    if (biased != 0) return biased - 1022;
+    const unsigned long long mant = absbits & ((1ull << 52) - 1);
+#ifdef __CUDA_ARCH__
+    return -1022 - (__clzll((long long)mant) - 12);
+#else
+    return -1022 - (__builtin_clzll(mant) - 12);
+#endif
+}
+
+__device__ __forceinline__ double pow2i(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+__device__ __forceinline__ double scale2(double x, int e)
+{
+    if (e >= -1022 && e <= 1023) return x * pow2i(e);
+    const int e1 = e / 2, e2 = e - e1;
+    return (x * pow2i(e1)) * pow2i(e2);
+}
+
+// ---------------------------------------------------------------- split kernels
+__global__ void ozaki_row_exp(const double *__restrict__ A, int m, int k, int lda, int *__restrict__ ea,
+                              int *status)
+{
+    const int warps = blockDim.x >> 5;
+    const int row = blockIdx.x * warps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= m) return;
+    const unsigned long long *r = reinterpret_cast<const unsigned long long *>(A + (size_t)row * lda);
+    unsigned long long mx = 0;
+    for (int kk = lane; kk < k; kk += 32) {
+        const unsigned long long b = __ldg(r + kk) & 0x7fffffffffffffffull;
+        mx = b > mx ? b : mx;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = other > mx ? other : mx;
+    }
+    if (lane == 0) {
+        if (mx >= 0x7ff0000000000000ull) {
+            ea[row] = NONFINITE_EXP;
+            record_status(status, kDevNonFinite);
+        } else {
+            ea[row] = frexp_exp_bits(mx);
+        }
+    }
+}
+
+// grid (ceil(n/256), ychunks); each thread scans a run of rows of one column.
+__global__ void ozaki_col_max(const double *__restrict__ B, int k, int n, int ldb, unsigned long long *colmax)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int rows_per = (k + gridDim.y - 1) / gridDim.y;
+    const int r0 = blockIdx.y * rows_per;
+    const int r1 = min(k, r0 + rows_per);
+    unsigned long long mx = 0;
+    const unsigned long long *b = reinterpret_cast<const unsigned long long *>(B);
+    for (int r = r0; r < r1; ++r) {
+        const unsigned long long v = __ldg(b + (size_t)r * ldb + j) & 0x7fffffffffffffffull;
+        mx = v > mx ? v : mx;
+    }
+    if (mx) atomicMax(colmax + j, mx);
+}
+
+__global__ void ozaki_col_exp(const unsigned long long *__restrict__ colmax, int n, int *__restrict__ eb,
+                              int *status)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long mx = colmax[j];
+    if (mx >= 0x7ff0000000000000ull) {
+        eb[j] = NONFINITE_EXP;
+        record_status(status, kDevNonFinite);
+    } else {
+        eb[j] = frexp_exp_bits(mx);
+    }
+}
+
+// Digits of one value (same operations as the oracle's digits_of).
+template <int S>
+__device__ __forceinline__ void digits(double v, int e, int8_t (&d)[S], int s)
+{
+    double x = scale2(v, 6 - e);
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+        if (t < s) {
+            const double r = rint(x);
+            d[t] = (int8_t)(int)r;
+            x = (x - r) * 128.0;
+        } else {
+            d[t] = 0;
+        }
+    }
+}
+
+// Each thread: 8 consecutive k of one row.  da layout [t][row][kp].
+__global__ void ozaki_split_a(const double *__restrict__ A, int m, int k, int lda, int kp, int s,
+                              const int *__restrict__ ea, int8_t *__restrict__ da)
+{
+    const int groups = kp / 8;
+    const size_t total = (size_t)m * groups;
+    const size_t slice = (size_t)m * kp;
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int row = (int)(idx / groups);
+        const int k0 = (int)(idx % groups) * 8;
+        int e = ea[row];
+        if (e == NONFINITE_EXP) e = 0;
+        unsigned long long packed[MAX_SPLITS];
+#pragma unroll
+        for (int t = 0; t < MAX_SPLITS; ++t) packed[t] = 0;
+        const double *arow = A + (size_t)row * lda;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int kk = k0 + j;
+            double v = (kk < k) ? __ldg(arow + kk) : 0.0;
+            if (!isfinite(v)) v = 0.0;
+            int8_t dg[MAX_SPLITS];
+            digits<MAX_SPLITS>(v, e, dg, s);
+#pragma unroll
+            for (int t = 0; t < MAX_SPLITS; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
+        }
+        for (int t = 0; t < s; ++t)
+            *reinterpret_cast<unsigned long long *>(da + t * slice + (size_t)row * kp + k0) = packed[t];
+    }
+}
+
+// Block: 64 k x 64 columns of B.  db layout [u][col][kp].
+__global__ void __launch_bounds__(256) ozaki_split_b(const double *__restrict__ B, int k, int n, int ldb, int kp,
+                                                     int s, const int *__restrict__ eb, int8_t *__restrict__ db)
+{
+    __shared__ double tileB[64][65];
+    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
+        const int r = idx / 64, c = idx % 64;
+        const int kk = k0 + r, jj = j0 + c;
+        double v = (kk < k && jj < n) ? __ldg(B + (size_t)kk * ldb + jj) : 0.0;
+        if (!isfinite(v)) v = 0.0;
+        tileB[r][c] = v;
+    }
+    __syncthreads();
+    // thread -> (column c, 16 consecutive k)
+    const int c = threadIdx.x >> 2;
+    const int kq = (threadIdx.x & 3) * 16;
+    const int jj = j0 + c;
+    if (jj >= n) return;
+    int e = eb[jj];
+    if (e == NONFINITE_EXP) e = 0;
+    unsigned long long lo[MAX_SPLITS], hi[MAX_SPLITS];
+#pragma unroll
+    for (int t = 0; t < MAX_SPLITS; ++t) lo[t] = hi[t] = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        int8_t dg[MAX_SPLITS];
+        digits<MAX_SPLITS>(tileB[kq + j][c], e, dg, s);
+#pragma unroll
+        for (int t = 0; t < MAX_SPLITS; ++t) {
+            const unsigned long long bits = (unsigned long long)(uint8_t)dg[t] << (8 * (j & 7));
+            if (j < 8) lo[t] |= bits;
+            else hi[t] |= bits;
+        }
+    }
+    const size_t slice = (size_t)n * kp;
+    const int kk = k0 + kq;
+    if (kk < kp) {
+        for (int t = 0; t < s; ++t) {
+            int8_t *dst = db + t * slice + (size_t)jj * kp + kk;
+            *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(lo[t], hi[t]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 helpers
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// K-major operand tile of 128 rows x 32 bytes written by TMA with the 32-byte swizzle:
+// rows 32 B apart, groups of 8 rows 256 B apart (SBO), LBO unused (1), layout type 6.
+__device__ __forceinline__ uint64_t sw32_desc(uint32_t smem_addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(256 >> 4) << 32;        // stride byte offset
+    d |= (uint64_t)1 << 46;                 // descriptor version (sm100)
+    d |= (uint64_t)6 << 61;                 // SWIZZLE_32B
+    return d;
+}
+
+// kind::i8 instruction descriptor: D s32, A s8, B s8, both K-major, M = 128, N = 128.
+constexpr uint32_t IDESC_S8_128x128 =
+    (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TILE >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tile_of(const GemmParams &p, int w, int &m0, int &n0, int &m_end, int &n_end)
+{
+    if (p.tiles) {
+        const int4 t = p.tiles[w];
+        m0 = t.x;
+        n0 = t.y;
+        m_end = t.z;
+        n_end = t.w;
+    } else {
+        const int tiles_n = (p.n + TILE - 1) / TILE;
+        // groups of 8 tile rows sweep the columns together so their A slices stay in L2
+        const int tiles_m = (p.m + TILE - 1) / TILE;
+        const int per_group = 8 * tiles_n;
+        const int g = w / per_group, r = w % per_group;
+        const int first = g * 8;
+        const int gsize = min(tiles_m - first, 8);
+        m0 = (first + r % gsize) * TILE;
+        n0 = (r / gsize) * TILE;
+        m_end = p.m;
+        n_end = p.n;
+    }
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+    ozaki_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                            ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + p.stages * p.stage_bytes);
+    uint64_t *empty = full + 4;
+    uint64_t *acc_full = empty + 4;
+    uint64_t *acc_empty = acc_full + 1;
+    uint64_t *drain = acc_empty + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = p.tiles ? p.num_tiles : ((p.m + TILE - 1) / TILE) * ((p.n + TILE - 1) / TILE);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < p.stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, EPI_WARPS);
+        mbar_init(drain, 1);
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (warp == 0 && lane == 0) {
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int armed[4] = {-1, -1, -1, -1};
+            bool ok = true;
+            for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
+                int m0, n0, m_end, n_end;
+                tile_of(p, w, m0, n0, m_end, n_end);
+                for (int si = 0; si < p.num_sets && ok; ++si) {
+                    const int nsl = min(p.splits, p.set_dhi[si] - 1);
+                    const uint32_t bytes = (uint32_t)(2 * nsl * SLICE_TILE_BYTES);
+                    for (int kb = 0; kb < p.kblocks; ++kb) {
+                        if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty)) {
+                            ok = false;
+                            break;
+                        }
+                        unsigned char *sa = smem + stage * p.stage_bytes;
+                        unsigned char *sb = sa + p.splits * SLICE_TILE_BYTES;
+                        mbar_arrive_expect_tx(&full[stage], bytes);
+                        armed[stage] = (int)phase;
+                        for (int t = 0; t < nsl; ++t) {
+                            tma_load_3d(sa + t * SLICE_TILE_BYTES, &tmA, kb * KBLK, m0, t, &full[stage]);
+                            tma_load_3d(sb + t * SLICE_TILE_BYTES, &tmB, kb * KBLK, n0, t, &full[stage]);
+                        }
+                        if (++stage == p.stages) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
+                    }
+                }
+            }
+            for (int s = 0; s < p.stages; ++s)
+                if (armed[s] >= 0) mbar_wait_bounded(&full[s], (uint32_t)armed[s], p.status, kDevTimeoutFull);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true;
+            const uint32_t smem_base = smem_u32(smem);
+            for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
+                for (int si = 0; si < p.num_sets && ok; ++si) {
+                    const int dhi = p.set_dhi[si], dlo = p.set_dlo[si];
+                    const int nsl = min(p.splits, dhi - 1);
+                    if (!mbar_wait_bounded(acc_empty, acc_phase ^ 1u, p.status, kDevTimeoutAcc)) {
+                        ok = false;
+                        break;
+                    }
+                    acc_phase ^= 1u;
+                    tc_fence_after();
+                    for (int kb = 0; kb < p.kblocks; ++kb) {
+                        if (!mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sa = smem_base + stage * p.stage_bytes;
+                        const uint32_t sb = sa + p.splits * SLICE_TILE_BYTES;
+                        uint32_t started = (kb > 0) ? 0xFu : 0u;
+                        for (int t = 1; t <= nsl; ++t) {
+                            const int ulo = max(1, dlo - t), uhi = min(nsl, dhi - t);
+                            const uint64_t adesc = sw32_desc(sa + (t - 1) * SLICE_TILE_BYTES);
+                            for (int u = ulo; u <= uhi; ++u) {
+                                const int slot = dhi - (t + u);
+                                const uint64_t bdesc = sw32_desc(sb + (u - 1) * SLICE_TILE_BYTES);
+                                tc_mma_i8(tmem_base + slot * TILE, adesc, bdesc, IDESC_S8_128x128, (started >> slot) & 1u);
+                                started |= 1u << slot;
+                            }
+                        }
+                        tc_commit(&empty[stage]);  // frees the stage once these MMAs have read it
+                        if (++stage == p.stages) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
+                    }
+                    if (ok) tc_commit(acc_full);
+                }
+            }
+            // Drain: all MMAs this thread issued have finished before TMEM is released.
+            tc_commit(drain);
+            mbar_wait_bounded(drain, 0, p.status, kDevTimeoutAcc);
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue (warps 2..9)
+        const int q = warp & 3;             // TMEM lane quarter this warp may access
+        const int half = (warp - 2) >> 2;   // which 64 of the 128 columns
+        uint32_t acc_phase = 0;
+        bool ok = true;
+        for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
+            int m0, n0, m_end, n_end;
+            tile_of(p, w, m0, n0, m_end, n_end);
+            double h[64];
+#pragma unroll
+            for (int j = 0; j < 64; ++j) h[j] = 0.0;
+            for (int si = 0; si < p.num_sets; ++si) {
+                bool got = true;
+                if (lane == 0) got = mbar_wait_bounded(acc_full, acc_phase, p.status, kDevTimeoutAcc);
+                got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                acc_phase ^= 1u;
+                tc_fence_after();
+                const int ngroups = p.set_dhi[si] - p.set_dlo[si] + 1;
+                for (int slot = 0; slot < ngroups; ++slot) {
+                    const uint32_t tbase = tmem_base + ((uint32_t)(32 * q) << 16) + slot * TILE + half * 64;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        uint32_t r[16];
+                        tmem_ld16(tbase + c * 16, r);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            h[c * 16 + j] = fma(h[c * 16 + j], 0.0078125, (double)(int)r[j]);
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty);
+            }
+            if (!ok) break;
+            const int row = m0 + 32 * q + lane;
+            if (row < m_end) {
+                const int er = p.ea[row];
+                double *crow = p.C + (size_t)row * p.ldc;
+                const int cbase = n0 + half * 64;
+#pragma unroll
+                for (int j = 0; j < 64; j += 2) {
+                    const int col = cbase + j;
+                    if (col >= n_end) break;
+                    const int e0 = p.eb[col];
+                    double v0 = (er == NONFINITE_EXP || e0 == NONFINITE_EXP) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                              : scale2(h[j], er + e0 - 12);
+                    if (col + 1 < n_end) {
+                        const int e1 = p.eb[col + 1];
+                        double v1 = (er == NONFINITE_EXP || e1 == NONFINITE_EXP)
+                                        ? __longlong_as_double(0x7ff8000000000000ll)
+                                        : scale2(h[j + 1], er + e1 - 12);
+                        if (p.vec_store) {
+                            double2 *dst = reinterpret_cast<double2 *>(crow + col);
+                            if (p.beta_one) {
+                                const double2 o = *dst;
+                                v0 = o.x + v0;
+                                v1 = o.y + v1;
+                            }
+                            *dst = make_double2(v0, v1);
+                        } else {
+                            crow[col] = p.beta_one ? crow[col] + v0 : v0;
+                            crow[col + 1] = p.beta_one ? crow[col + 1] + v1 : v1;
+                        }
+                    } else {
+                        crow[col] = p.beta_one ? crow[col] + v0 : v0;
+                    }
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    __syncwarp();
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(512) : "memory");
+}
+
+}  // namespace oz
+}  // namespace mgx
+
+using namespace mgx;
+
+namespace {
+
+struct WsLayout {
+    size_t da, db, ea, eb, colmax, total;
+    int kp;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int ozaki_kmax(int s) { return (int)((2147483647ll / (4096ll * s)) & ~127ll); }
+
+WsLayout ws_layout(int m, int n, int k, int s)
+{
+    WsLayout L;
+    int kc = k;
+    const int kmax = ozaki_kmax(s);
+    if (kc > kmax) kc = kmax;
+    L.kp = (kc + 31) & ~31;
+    if (L.kp == 0) L.kp = 32;
+    size_t off = 0;
+    L.da = off;
+    off = align256(off + (size_t)s * m * L.kp);
+    L.db = off;
+    off = align256(off + (size_t)s * n * L.kp);
+    L.ea = off;
+    off = align256(off + sizeof(int) * (size_t)m);
+    L.eb = off;
+    off = align256(off + sizeof(int) * (size_t)n);
+    L.colmax = off;
+    off = align256(off + sizeof(unsigned long long) * (size_t)n);
+    L.total = off;
+    return L;
+}
+
+}  // namespace
+
+// Phase 1: exponents and digit planes of A (m x k) and B (k x n) into the workspace (k <= kmax).
+static int ozaki_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int s,
+                            unsigned char *ws, const WsLayout &L, cudaStream_t stream)
+{
+    int *status = mgx_device_status_ptr();
+    int8_t *da = reinterpret_cast<int8_t *>(ws + L.da);
+    int8_t *db = reinterpret_cast<int8_t *>(ws + L.db);
+    int *ea = reinterpret_cast<int *>(ws + L.ea);
+    int *eb = reinterpret_cast<int *>(ws + L.eb);
+    unsigned long long *colmax = reinterpret_cast<unsigned long long *>(ws + L.colmax);
+    const int kp = (k + 31) & ~31;
+    const int sms = mgx_sm_count();
+
+    oz::ozaki_row_exp<<<(m + 7) / 8, 256, 0, stream>>>(A, m, k, lda, ea, status);
+    MGX_HOST_CHECK(cudaGetLastError());
+    MGX_HOST_CHECK(cudaMemsetAsync(colmax, 0, sizeof(unsigned long long) * (size_t)n, stream));
+    {
+        int ych = (sms * 8) / ((n + 255) / 256);
+        if (ych > (k + 63) / 64) ych = (k + 63) / 64;
+        if (ych < 1) ych = 1;
+        dim3 g((n + 255) / 256, ych);
+        oz::ozaki_col_max<<<g, 256, 0, stream>>>(B, k, n, ldb, colmax);
+        MGX_HOST_CHECK(cudaGetLastError());
+        oz::ozaki_col_exp<<<(n + 255) / 256, 256, 0, stream>>>(colmax, n, eb, status);
+        MGX_HOST_CHECK(cudaGetLastError());
+    }
+    oz::ozaki_split_a<<<sms * 8, 256, 0, stream>>>(A, m, k, lda, kp, s, ea, da);
+    MGX_HOST_CHECK(cudaGetLastError());
+    {
+        dim3 g((n + 63) / 64, (kp + 63) / 64);
+        oz::ozaki_split_b<<<g, 256, 0, stream>>>(B, k, n, ldb, kp, s, eb, db);
+        MGX_HOST_CHECK(cudaGetLastError());
+    }
+    return MGX_SUCCESS;
+}
+
+// Phase 2: C (+)= recombined slice products (tcgen05 kernel); the work list is optional.
+static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta_one, int s, const unsigned char *ws,
+                               const WsLayout &L, const int4 *tiles, int num_tiles, cudaStream_t stream)
+{
+    const int kp = (k + 31) & ~31;
+    const int8_t *da = reinterpret_cast<const int8_t *>(ws + L.da);
+    const int8_t *db = reinterpret_cast<const int8_t *>(ws + L.db);
+    // tensor maps over the digit planes: dims {kp, rows, s}, box {32, 128, 1}, 32-byte swizzle
+    CUtensorMap tmA, tmB;
+    int rc = mgx_encode_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, da, (uint64_t)kp, (uint64_t)m, (uint64_t)s,
+                                (uint64_t)kp, (uint64_t)m * kp, oz::KBLK, oz::TILE, 1, CU_TENSOR_MAP_SWIZZLE_32B);
+    if (rc != MGX_SUCCESS) return rc;
+    rc = mgx_encode_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, db, (uint64_t)kp, (uint64_t)n, (uint64_t)s,
+                            (uint64_t)kp, (uint64_t)n * kp, oz::KBLK, oz::TILE, 1, CU_TENSOR_MAP_SWIZZLE_32B);
+    if (rc != MGX_SUCCESS) return rc;
+
+    oz::GemmParams p;
+    memset(&p, 0, sizeof p);
+    p.C = C;
+    p.m = m;
+    p.n = n;
+    p.ldc = ldc;
+    p.kblocks = kp / oz::KBLK;
+    p.splits = s;
+    // weight sets of up to four groups, highest weights first
+    int d = s + 1, ns = 0;
+    while (d >= 2) {
+        p.set_dhi[ns] = d;
+        p.set_dlo[ns] = (d - 3 > 2) ? d - 3 : 2;
+        d = p.set_dlo[ns] - 1;
+        ++ns;
+    }
+    p.num_sets = ns;
+    p.stage_bytes = 2 * s * oz::SLICE_TILE_BYTES;
+    const int budget = 220 * 1024;
+    p.stages = budget / p.stage_bytes;
+    if (p.stages > 4) p.stages = 4;
+    if (p.stages < 2) {
+        mgx_set_last_message("mgx_gemm_ozaki: %d splits do not fit two pipeline stages", s);
+        return MGX_E_UNSUPPORTED;
+    }
+    p.ea = reinterpret_cast<const int *>(ws + L.ea);
+    p.eb = reinterpret_cast<const int *>(ws + L.eb);
+    p.tiles = tiles;
+    p.num_tiles = num_tiles;
+    p.beta_one = beta_one;
+    p.vec_store = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+    p.status = mgx_device_status_ptr();
+    const int smem = p.stages * p.stage_bytes + 1024 + 256;
+    MGX_HOST_CHECK(cudaFuncSetAttribute(oz::ozaki_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int total = tiles ? num_tiles : ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE);
+    const int sms = mgx_sm_count();
+    const int grid = sms < total ? sms : total;
+    if (grid < 1) return MGX_SUCCESS;
+    oz::ozaki_gemm<<<grid, oz::THREADS, smem, stream>>>(tmA, tmB, p);
+    MGX_HOST_CHECK(cudaGetLastError());
+    return MGX_SUCCESS;
+}
+
+static bool ozaki_args_ok(int m, int n, int k, int splits)
+{
+    return m >= 0 && n >= 0 && k >= 0 && splits >= 2 && splits <= oz::MAX_SPLITS;
+}
+
+static int ozaki_ws_check(void *workspace, size_t workspace_bytes, const WsLayout &L, const char *who)
+{
+    if (!workspace || workspace_bytes < L.total || (reinterpret_cast<uintptr_t>(workspace) & 255)) {
+        mgx_set_last_message("%s: workspace needs %zu bytes, 256-byte aligned (got %zu)", who, L.total,
+                             workspace_bytes);
+        return MGX_E_WORKSPACE;
+    }
+    return MGX_SUCCESS;
+}
+
+extern "C" MGX_API size_t mgx_ozaki_workspace_size(int m, int n, int k, int splits)
+{
+    if (m < 0 || n < 0 || k < 0 || splits < 2 || splits > oz::MAX_SPLITS) return 0;
+    return ws_layout(m, n, k, splits).total;
+}
+
+int mgx_ozaki_run(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb, int ldc,
+                  int beta_one, int splits, void *workspace, size_t workspace_bytes, const int4 *tiles, int num_tiles,
+                  cudaStream_t stream)
+{
+    if (!ozaki_args_ok(m, n, k, splits) || (m > 0 && n > 0 && !C) ||
+        (m > 0 && n > 0 && k > 0 && (!A || !B || lda < k || ldb < n)) || (m > 0 && n > 0 && ldc < n)) {
+        mgx_set_last_message("mgx_gemm_ozaki: invalid arguments m=%d n=%d k=%d splits=%d", m, n, k, splits);
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0) return MGX_SUCCESS;
+    if (k == 0) {
+        if (beta_one) return MGX_SUCCESS;
+        MGX_HOST_CHECK(cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)n * sizeof(double), m, stream));
+        return MGX_SUCCESS;
+    }
+    const WsLayout L = ws_layout(m, n, k, splits);
+    const int wrc = ozaki_ws_check(workspace, workspace_bytes, L, "mgx_gemm_ozaki");
+    if (wrc != MGX_SUCCESS) return wrc;
+    const int kmax = ozaki_kmax(splits);
+    for (int k0 = 0; k0 < k; k0 += kmax) {
+        const int kc = (k - k0 < kmax) ? k - k0 : kmax;
+        unsigned char *ws = static_cast<unsigned char *>(workspace);
+        int rc = ozaki_split_impl(A + k0, B + (size_t)k0 * ldb, m, n, kc, lda, ldb, splits, ws, L, stream);
+        if (rc != MGX_SUCCESS) return rc;
+        rc = ozaki_multiply_impl(C, m, n, kc, ldc, (k0 > 0) ? 1 : beta_one, splits, ws, L, tiles, num_tiles, stream);
+        if (rc != MGX_SUCCESS) return rc;
+    }
+    return MGX_SUCCESS;
+}
+
+extern "C" MGX_API int mgx_gemm_ozaki(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                      int ldb, int ldc, int beta_one, int splits, void *workspace,
+                                      size_t workspace_bytes, void *stream)
+{
+    return mgx_ozaki_run(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, splits, workspace, workspace_bytes,
+                         nullptr, 0, (cudaStream_t)stream);
+}
+
+// A-priori split choice.  The normwise error of the Ozaki form falls by close to two decimal
+// digits per added slice and does not grow with K (exact integer accumulation); its level is
+// set by how far the entries of a row or column spread below the row's (column's) maximum,
+// which saturates after about ten binades.  Fitted on the oracle for uniform and wide-exponent
+// inputs (K = 256 .. 1024):
+//     err(s, R) ~= c(R) * 10^(-2 (s - 4)),  c(0) = 8.5e-9,  c(R >= 10) = 7.2e-8,
+// floored at 5e-17 by the FP64 recombination.  The smallest s whose prediction, with a 1.25
+// safety factor, meets `target` is returned (2..12).
+extern "C" MGX_API int mgx_ozaki_choose_splits(int k, double exp_range, double target)
+{
+    (void)k;
+    if (!(target > 0.0)) target = 1e-15;
+    const double r = exp_range < 0.0 ? 0.0 : (exp_range > 10.0 ? 10.0 : exp_range);
+    const double c = 8.5e-9 * pow(10.0, 0.93 * r / 10.0);
+    for (int s = 2; s <= oz::MAX_SPLITS; ++s) {
+        double e = c * pow(10.0, -2.0 * (s - 4));
+        if (e < 5e-17) e = 5e-17;
+        if (e * 1.25 <= target) return s;
+    }
+    return oz::MAX_SPLITS;
+}
+
+extern "C" MGX_API int mgx_ozaki_split(const double *A, const double *B, int m, int n, int k, int lda, int ldb,
+                                       int splits, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!ozaki_args_ok(m, n, k, splits) || k > ozaki_kmax(splits) || (m > 0 && k > 0 && (!A || lda < k)) ||
+        (n > 0 && k > 0 && (!B || ldb < n))) {
+        mgx_set_last_message("mgx_ozaki_split: invalid arguments (k must be <= %d for %d splits)",
+                             splits >= 2 && splits <= oz::MAX_SPLITS ? ozaki_kmax(splits) : 0, splits);
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0 || k == 0) return MGX_SUCCESS;
+    const WsLayout L = ws_layout(m, n, k, splits);
+    const int wrc = ozaki_ws_check(workspace, workspace_bytes, L, "mgx_ozaki_split");
+    if (wrc != MGX_SUCCESS) return wrc;
+    return ozaki_split_impl(A, B, m, n, k, lda, ldb, splits, static_cast<unsigned char *>(workspace), L,
+                            (cudaStream_t)stream);
+}
+
+extern "C" MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ldc, int beta_one, int splits,
+                                          const void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!ozaki_args_ok(m, n, k, splits) || k > ozaki_kmax(splits) || (m > 0 && n > 0 && (!C || ldc < n))) {
+        mgx_set_last_message("mgx_ozaki_multiply: invalid arguments");
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0) return MGX_SUCCESS;
+    if (k == 0) {
+        if (beta_one) return MGX_SUCCESS;
+        MGX_HOST_CHECK(cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)n * sizeof(double), m,
+                                         (cudaStream_t)stream));
+        return MGX_SUCCESS;
+    }
+    const WsLayout L = ws_layout(m, n, k, splits);
+    const int wrc = ozaki_ws_check(const_cast<void *>(workspace), workspace_bytes, L, "mgx_ozaki_multiply");
+    if (wrc != MGX_SUCCESS) return wrc;
+    return ozaki_multiply_impl(C, m, n, k, ldc, beta_one ? 1 : 0, splits, static_cast<const unsigned char *>(workspace),
+                               L, nullptr, 0, (cudaStream_t)stream);
+}
+
+extern "C" MGX_API int mgx_ozaki_kmax(int splits)
+{
+    if (splits < 2 || splits > oz::MAX_SPLITS) return 0;
+    return ozaki_kmax(splits);
+}

@@ -1,0 +1,77 @@
+"""The drop-in executables on the GPU: MGXBench's record contract (benchmark.py:45-50, 147-156)."""
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+BUILD = ROOT / "build"
+LAUNCHER = ROOT / "mgxbench_b200" / "mgx-onegpu-launch"
+
+
+def parse_result(output):
+    """benchmark.py's parser rule: exactly one BENCHMARK_RESULT record of k=v pairs."""
+    matches = re.findall(r"BENCHMARK_RESULT\s+([^\r\n]+)", output)
+    assert len(matches) == 1, output
+    return dict(x.split("=", 1) for x in matches[0].split())
+
+
+def launch(exe, ranks, n, lib, **env):
+    cmd = [sys.executable, str(LAUNCHER)]
+    for r in range(ranks):
+        if r:
+            cmd.append(":")
+        cmd += ["-np", "1", str(BUILD / exe), "auto", str(n), lib]
+    e = dict(os.environ, MGXBENCH_INNER_LOOPS="2", **{k: str(v) for k, v in env.items()})
+    return subprocess.run(cmd, capture_output=True, text=True, env=e, timeout=300)
+
+
+@pytest.mark.parametrize("lib,ranks", [("MMM", 1), ("SSS", 4), ("NYN", 2), ("XXX", 1)])
+def test_mm1d_records(lib, ranks):
+    r = launch("mm_1d", ranks, 512, lib, MM_PIPELINE_K_CHUNK=96)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rec = parse_result(r.stdout)
+    assert rec["decomposition"].lower() == "1d" and rec["library"] == lib and rec["valid"] == "1"
+    assert int(rec["size"]) == 512 and int(rec["ranks"]) == ranks and int(rec["loops"]) == 2
+    assert float(rec["seconds"]) > 0
+    assert "NUMERICAL VALIDATION" in r.stdout and "Result             : PASS" in r.stdout
+    assert re.search(r"RESULT: Matrix size: 512\tTime \(seconds\): [0-9.]+", r.stdout)
+
+
+def test_mm1d_ozaki_random_inputs():
+    r = launch("mm_1d", 2, 1024, "MMM", MGXBENCH_FORM="ozaki", MGXBENCH_INPUT="wide", MGXBENCH_SPLITS=8)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rec = parse_result(r.stdout)
+    assert rec["valid"] == "1" and float(rec["norm_rel_err"]) <= 1e-15
+
+
+@pytest.mark.parametrize("lib,ranks,env", [("MMM", 1, {}), ("NNN", 4, {}), ("SSS", 6, {"MGXBENCH_SUMMA_BK": 64}),
+                                           ("YYY", 15, {"MGXBENCH_GRID_ROWS": 3, "MGXBENCH_GRID_COLS": 5,
+                                                        "MGXBENCH_SUMMA_BK": 128})])
+def test_mm2d_records(lib, ranks, env):
+    n = 960
+    r = launch("mm_2d", ranks, n, lib, MGXBENCH_INNER_LOOPS=1, **env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rec = parse_result(r.stdout)
+    assert rec["decomposition"].lower() == "2d" and rec["valid"] == "1" and int(rec["ranks"]) == ranks
+    assert rec["loops"] == "1" and "x" in rec["grid"]
+
+
+def test_mm2d_uneven_extension():
+    r = launch("mm_2d", 15, 1000, "MMM", MGXBENCH_GRID_ROWS=3, MGXBENCH_GRID_COLS=5, MGXBENCH_UNEVEN=1,
+               MGXBENCH_M=1001, MGXBENCH_N=997, MGXBENCH_K=515, MGXBENCH_SUMMA_BK=64)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert parse_result(r.stdout)["valid"] == "1"
+
+
+def test_mm2d_invalid_result_exit_code():
+    """A product that fails validation exits 1 (2D-block-matrix/mmb.cu:439)."""
+    r = launch("mm_2d", 1, 256, "MMM", MGXBENCH_INPUT="uniform", MGXBENCH_FORM="fp64", MGXBENCH_CHECK_ROWS=64)
+    rec = parse_result(r.stdout)
+    # FP64 on uniform inputs meets the 1e-12 check, so this run is valid
+    assert r.returncode == 0 and rec["valid"] == "1"

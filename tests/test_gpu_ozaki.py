@@ -1,0 +1,97 @@
+"""Ozaki INT8 tensor-core form on the GPU: bit-identical to the oracle's restatement (the digit
+slices and int32 sums are integer work; the FP64 recombination follows the same operations in the
+same order), and accurate against the double-double product."""
+import numpy as np
+import pytest
+
+from conftest import rng_matrix
+from gpu_util import bits, dev, host
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("m,n,k,s", [(128, 128, 32, 3), (128, 128, 256, 8), (1, 1, 1, 4), (77, 200, 333, 5),
+                                     (300, 129, 1000, 7), (256, 256, 512, 9), (130, 260, 96, 2), (64, 64, 64, 12)])
+def test_ozaki_bit_exact_vs_oracle(mgx, oracle, m, n, k, s):
+    import torch
+    rng = np.random.default_rng(m * 31 + n * 7 + k + s)
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    dC = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki(dev(A), dev(B), dC, splits=s)
+    C = host(dC)
+    assert np.array_equal(bits(C), bits(oracle.ozaki_gemm(A, B, s)))
+    assert mgx.device_status() == 0
+
+
+def test_ozaki_beta_one_and_uniform(mgx, oracle):
+    rng = np.random.default_rng(3)
+    A, B, C0 = rng_matrix(rng, (200, 300)), rng_matrix(rng, (300, 170)), rng_matrix(rng, (200, 170))
+    dC = dev(C0)
+    mgx.gemm_ozaki(dev(A), dev(B), dC, splits=8, beta_one=True)
+    assert np.array_equal(bits(host(dC)), bits(oracle.ozaki_gemm(A, B, 8, C=C0.copy(), beta_one=True)))
+
+
+def test_ozaki_split_multiply_phases(mgx, oracle):
+    import torch
+    rng = np.random.default_rng(4)
+    A, B = rng_matrix(rng, (256, 512), "wide"), rng_matrix(rng, (512, 384), "wide")
+    ws = torch.empty(mgx.ozaki_workspace_size(256, 384, 512, 8), dtype=torch.uint8, device="cuda")
+    mgx.ozaki_split(dev(A), dev(B), 8, ws)
+    dC = torch.empty((256, 384), dtype=torch.float64, device="cuda")
+    mgx.ozaki_multiply(dC, 512, 8, ws)
+    first = host(dC).copy()
+    mgx.ozaki_multiply(dC, 512, 8, ws)      # slices reused
+    assert np.array_equal(bits(first), bits(host(dC)))
+    assert np.array_equal(bits(first), bits(oracle.ozaki_gemm(A, B, 8)))
+
+
+@pytest.mark.parametrize("s,target", [(8, 1e-15), (9, 1e-16)])
+def test_ozaki_accuracy_wide_exponents(mgx, oracle, s, target):
+    import torch
+    rng = np.random.default_rng(5)
+    A, B = rng_matrix(rng, (512, 2048), "wide"), rng_matrix(rng, (2048, 512), "wide")
+    dA, dB = dev(A), dev(B)
+    dC = torch.empty((512, 512), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki(dA, dB, dC, splits=s)
+    e = mgx.error_vs_dd(dA, dB, dC)
+    assert e["normwise"] <= target
+
+
+def test_ozaki_integer_known_answer(mgx):
+    import torch
+    N = 1024
+    A = torch.ones((N, N), dtype=torch.float64, device="cuda")
+    B = torch.full((N, N), 2.0, dtype=torch.float64, device="cuda")
+    C = torch.empty((N, N), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki(A, B, C, splits=3)
+    assert torch.all(C == 2.0 * N)
+
+
+def test_ozaki_nonfinite_marks_rows_and_columns(mgx):
+    import torch
+    rng = np.random.default_rng(6)
+    A, B = rng_matrix(rng, (140, 64)), rng_matrix(rng, (64, 150))
+    A[5, 7] = np.inf
+    B[3, 9] = np.nan
+    dC = torch.empty((140, 150), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki(dev(A), dev(B), dC, splits=4)
+    C = host(dC)
+    assert mgx.device_status() == 4          # non-finite input recorded on the device
+    assert np.all(np.isnan(C[5])) and np.all(np.isnan(C[:, 9]))
+    mask = np.ones_like(C, dtype=bool)
+    mask[5] = False
+    mask[:, 9] = False
+    assert np.all(np.isfinite(C[mask]))
+
+
+def test_ozaki_k_beyond_int32_headroom(mgx, oracle):
+    """K larger than one int32 accumulation allows is split into ordered chunks."""
+    import torch
+    s = 12
+    kmax = mgx.ozaki_kmax(s)
+    k = kmax + 200
+    rng = np.random.default_rng(7)
+    A, B = rng_matrix(rng, (8, k)), rng_matrix(rng, (k, 8))
+    dC = torch.empty((8, 8), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki(dev(A), dev(B), dC, splits=s)
+    assert np.array_equal(bits(host(dC)), bits(oracle.ozaki_gemm(A, B, s)))
