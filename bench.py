@@ -114,7 +114,7 @@ def cpu_reference_rate(n: int, budget_s: float, threads: int = 0):
     from oracle import oracle as O
     rng = np.random.default_rng(1)
     B = rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-EXP_RANGE, EXP_RANGE + 1, (n, n)))
-    probe = 8
+    probe = 128
     A = rng.uniform(-1, 1, (probe, n))
     t0 = time.perf_counter()
     O.ab_multiply(A, B, threads=threads)

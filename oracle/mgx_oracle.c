@@ -72,62 +72,70 @@ static void chain_panel(const double *A, int lda, const double *B, int ldb, doub
                 for (int kk = 0; kk < kc; ++kk)
                     memcpy(Bp + ((size_t)jb * kc + kk) * 8, B + (size_t)(k0 + kk) * ldb + j0 + jb * 8,
                            8 * sizeof(double));
-#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
-            for (int i0 = 0; i0 < m; i0 += 4) {
-                const int mr = (m - i0 < 4) ? m - i0 : 4;
-                double areg[4][KC];
-                for (int r = 0; r < 4; ++r)
-                    for (int kk = 0; kk < kc; ++kk) {
-                        const int row = (r < mr) ? i0 + r : i0;
-                        areg[r][kk] = (k0 + kk < a_live) ? A[(size_t)row * lda + k0 + kk] : 0.0;
-                    }
-                for (int jb = 0; jb < nc8 / 8; ++jb) {
-                    const double *bp = Bp + (size_t)jb * kc * 8;
-                    double *pc = P + (size_t)i0 * ldp + j0 + jb * 8;
-                    if (mr == 4) {
-                        __m256d c00, c01, c10, c11, c20, c21, c30, c31;
-                        if (first) {
-                            c00 = c01 = c10 = c11 = c20 = c21 = c30 = c31 = _mm256_setzero_pd();
-                        } else {
-                            c00 = _mm256_loadu_pd(pc + 0 * ldp); c01 = _mm256_loadu_pd(pc + 0 * ldp + 4);
-                            c10 = _mm256_loadu_pd(pc + 1 * ldp); c11 = _mm256_loadu_pd(pc + 1 * ldp + 4);
-                            c20 = _mm256_loadu_pd(pc + 2 * ldp); c21 = _mm256_loadu_pd(pc + 2 * ldp + 4);
-                            c30 = _mm256_loadu_pd(pc + 3 * ldp); c31 = _mm256_loadu_pd(pc + 3 * ldp + 4);
-                        }
+            /* one work item = 4 rows x 64 columns of this panel (ragged columns go with jg == 0) */
+            const int iblocks = (m + 3) / 4;
+            const int jgroups = (nc8 / 8 + 7) / 8 > 0 ? (nc8 / 8 + 7) / 8 : 1;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4) collapse(2)
+            for (int ib = 0; ib < iblocks; ++ib) {
+                for (int jg = 0; jg < jgroups; ++jg) {
+                    const int i0 = ib * 4;
+                    const int mr = (m - i0 < 4) ? m - i0 : 4;
+                    double areg[4][KC];
+                    for (int r = 0; r < 4; ++r)
                         for (int kk = 0; kk < kc; ++kk) {
-                            const __m256d b0 = _mm256_load_pd(bp + kk * 8);
-                            const __m256d b1 = _mm256_load_pd(bp + kk * 8 + 4);
-                            __m256d a = _mm256_broadcast_sd(&areg[0][kk]);
-                            c00 = _mm256_fmadd_pd(a, b0, c00); c01 = _mm256_fmadd_pd(a, b1, c01);
-                            a = _mm256_broadcast_sd(&areg[1][kk]);
-                            c10 = _mm256_fmadd_pd(a, b0, c10); c11 = _mm256_fmadd_pd(a, b1, c11);
-                            a = _mm256_broadcast_sd(&areg[2][kk]);
-                            c20 = _mm256_fmadd_pd(a, b0, c20); c21 = _mm256_fmadd_pd(a, b1, c21);
-                            a = _mm256_broadcast_sd(&areg[3][kk]);
-                            c30 = _mm256_fmadd_pd(a, b0, c30); c31 = _mm256_fmadd_pd(a, b1, c31);
+                            const int row = (r < mr) ? i0 + r : i0;
+                            areg[r][kk] = (k0 + kk < a_live) ? A[(size_t)row * lda + k0 + kk] : 0.0;
                         }
-                        _mm256_storeu_pd(pc + 0 * ldp, c00); _mm256_storeu_pd(pc + 0 * ldp + 4, c01);
-                        _mm256_storeu_pd(pc + 1 * ldp, c10); _mm256_storeu_pd(pc + 1 * ldp + 4, c11);
-                        _mm256_storeu_pd(pc + 2 * ldp, c20); _mm256_storeu_pd(pc + 2 * ldp + 4, c21);
-                        _mm256_storeu_pd(pc + 3 * ldp, c30); _mm256_storeu_pd(pc + 3 * ldp + 4, c31);
-                    } else {
+                    for (int jb = jg * 8; jb < jg * 8 + 8 && jb < nc8 / 8; ++jb) {
+                        const double *bp = Bp + (size_t)jb * kc * 8;
+                        double *pc = P + (size_t)i0 * ldp + j0 + jb * 8;
+                        if (mr == 4) {
+                            __m256d c00, c01, c10, c11, c20, c21, c30, c31;
+                            if (first) {
+                                c00 = c01 = c10 = c11 = c20 = c21 = c30 = c31 = _mm256_setzero_pd();
+                            } else {
+                                c00 = _mm256_loadu_pd(pc + 0 * ldp); c01 = _mm256_loadu_pd(pc + 0 * ldp + 4);
+                                c10 = _mm256_loadu_pd(pc + 1 * ldp); c11 = _mm256_loadu_pd(pc + 1 * ldp + 4);
+                                c20 = _mm256_loadu_pd(pc + 2 * ldp); c21 = _mm256_loadu_pd(pc + 2 * ldp + 4);
+                                c30 = _mm256_loadu_pd(pc + 3 * ldp); c31 = _mm256_loadu_pd(pc + 3 * ldp + 4);
+                            }
+                            for (int kk = 0; kk < kc; ++kk) {
+                                const __m256d b0 = _mm256_load_pd(bp + kk * 8);
+                                const __m256d b1 = _mm256_load_pd(bp + kk * 8 + 4);
+                                __m256d a = _mm256_broadcast_sd(&areg[0][kk]);
+                                c00 = _mm256_fmadd_pd(a, b0, c00); c01 = _mm256_fmadd_pd(a, b1, c01);
+                                a = _mm256_broadcast_sd(&areg[1][kk]);
+                                c10 = _mm256_fmadd_pd(a, b0, c10); c11 = _mm256_fmadd_pd(a, b1, c11);
+                                a = _mm256_broadcast_sd(&areg[2][kk]);
+                                c20 = _mm256_fmadd_pd(a, b0, c20); c21 = _mm256_fmadd_pd(a, b1, c21);
+                                a = _mm256_broadcast_sd(&areg[3][kk]);
+                                c30 = _mm256_fmadd_pd(a, b0, c30); c31 = _mm256_fmadd_pd(a, b1, c31);
+                            }
+                            _mm256_storeu_pd(pc + 0 * ldp, c00); _mm256_storeu_pd(pc + 0 * ldp + 4, c01);
+                            _mm256_storeu_pd(pc + 1 * ldp, c10); _mm256_storeu_pd(pc + 1 * ldp + 4, c11);
+                            _mm256_storeu_pd(pc + 2 * ldp, c20); _mm256_storeu_pd(pc + 2 * ldp + 4, c21);
+                            _mm256_storeu_pd(pc + 3 * ldp, c30); _mm256_storeu_pd(pc + 3 * ldp + 4, c31);
+                        } else {
+                            for (int r = 0; r < mr; ++r)
+                                for (int c = 0; c < 8; ++c) {
+                                    double acc = first ? 0.0 : pc[(size_t)r * ldp + c];
+                                    for (int kk = 0; kk < kc; ++kk)
+                                        acc = fma(areg[r][kk], bp[kk * 8 + c], acc);
+                                    pc[(size_t)r * ldp + c] = acc;
+                                }
+                        }
+                    }
+                    if (jg == 0) {
+                        /* ragged columns */
                         for (int r = 0; r < mr; ++r)
-                            for (int c = 0; c < 8; ++c) {
-                                double acc = first ? 0.0 : pc[(size_t)r * ldp + c];
+                            for (int c = j0 + nc8; c < j0 + nc; ++c) {
+                                double acc = first ? 0.0 : P[(size_t)(i0 + r) * ldp + c];
                                 for (int kk = 0; kk < kc; ++kk)
-                                    acc = fma(areg[r][kk], bp[kk * 8 + c], acc);
-                                pc[(size_t)r * ldp + c] = acc;
+                                    acc = fma(areg[r][kk], B[(size_t)(k0 + kk) * ldb + c], acc);
+                                P[(size_t)(i0 + r) * ldp + c] = acc;
                             }
                     }
                 }
-                /* ragged columns */
-                for (int r = 0; r < mr; ++r)
-                    for (int c = j0 + nc8; c < j0 + nc; ++c) {
-                        double acc = first ? 0.0 : P[(size_t)(i0 + r) * ldp + c];
-                        for (int kk = 0; kk < kc; ++kk)
-                            acc = fma(areg[r][kk], B[(size_t)(k0 + kk) * ldb + c], acc);
-                        P[(size_t)(i0 + r) * ldp + c] = acc;
-                    }
             }
         }
         if (k == 0) {
