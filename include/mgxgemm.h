@@ -194,6 +194,27 @@ MGX_API int mgx_fill_matrix(double *X, int rows, int cols, int ld, int kind, dou
                             uint64_t seed, void *stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Learned cost model of the autotuner: a 3-layer FP32 MLP (6 -> 64 -> 64 -> 2, tanh) trained
+ * and evaluated on the GPU.  Inputs per sample (standardised by the caller): log2 M, log2 N,
+ * log2 K, input exponent range, tile shape id, split count.  Outputs: standardised log
+ * runtime and log10 normwise error.  No counterpart in MGXBench: it replaces the regression of
+ * autotuning/predictive.py:100-165.  All pointers are device pointers; stream-ordered.
+ * ------------------------------------------------------------------------------------------ */
+
+/* Number of floats in the parameter vector (W1 | b1 | W2 | b2 | W3 | b3). */
+MGX_API int mgx_mlp_param_count(void);
+/* Glorot-uniform weights from `seed`, zero biases. */
+MGX_API int mgx_mlp_init(float *params, uint64_t seed, void *stream);
+/* out[batch x 2] = MLP(X[batch x 6]). */
+MGX_API int mgx_mlp_forward(const float *X, int batch, const float *params, float *out, void *stream);
+/* grads = d loss / d params and *loss = sum_o w_o (out_o - Y_o)^2 / batch over the batch. */
+MGX_API int mgx_mlp_gradients(const float *X, const float *Y, const float *out_weights, int batch,
+                              const float *params, float *grads, float *loss, void *stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8); `step` counts from 1. */
+MGX_API int mgx_mlp_adam_step(float *params, const float *grads, float *m, float *v, int step, float lr,
+                              void *stream);
+
+/* ------------------------------------------------------------------------------------------
  * Library state
  * ------------------------------------------------------------------------------------------ */
 

@@ -77,6 +77,11 @@ EXPORTS = [
     ("mgx_last_error_message", ctypes.c_char_p, []),
     ("mgx_status_string", ctypes.c_char_p, [_i]),
     ("mgx_peak_fp64", _i, [_i, _i, ctypes.POINTER(_d)]),
+    ("mgx_mlp_param_count", _i, []),
+    ("mgx_mlp_init", _i, [_vp, _u64, _vp]),
+    ("mgx_mlp_forward", _i, [_vp, _i, _vp, _vp, _vp]),
+    ("mgx_mlp_gradients", _i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _vp]),
+    ("mgx_mlp_adam_step", _i, [_vp, _vp, _vp, _vp, _i, ctypes.c_float, _vp]),
 ]
 
 _lib = None
@@ -290,3 +295,40 @@ def peak_fp64(kind: int, iterations: int = 20000) -> float:
     out = ctypes.c_double()
     _check(lib().mgx_peak_fp64(kind, iterations, ctypes.byref(out)), "mgx_peak_fp64")
     return out.value
+
+
+# ------------------------------------------------------------------ learned cost model kernels
+def _check_f32(*ts):
+    import torch
+    for t in ts:
+        if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+            raise MgxError(-1, "argument", "MLP tensors must be contiguous float32 CUDA tensors")
+
+
+def mlp_param_count() -> int:
+    return int(lib().mgx_mlp_param_count())
+
+
+def mlp_init(params, seed: int = 0, stream=None):
+    _check_f32(params)
+    return _check(lib().mgx_mlp_init(_ptr(params), seed, _stream(stream)), "mgx_mlp_init")
+
+
+def mlp_forward(X, params, out=None, stream=None):
+    import torch
+    _check_f32(X, params)
+    out = torch.empty((X.shape[0], 2), dtype=torch.float32, device="cuda") if out is None else out
+    _check(lib().mgx_mlp_forward(_ptr(X), X.shape[0], _ptr(params), _ptr(out), _stream(stream)), "mgx_mlp_forward")
+    return out
+
+
+def mlp_gradients(X, Y, weights, params, grads, loss, stream=None):
+    _check_f32(X, Y, weights, params, grads, loss)
+    return _check(lib().mgx_mlp_gradients(_ptr(X), _ptr(Y), _ptr(weights), X.shape[0], _ptr(params), _ptr(grads),
+                                          _ptr(loss), _stream(stream)), "mgx_mlp_gradients")
+
+
+def mlp_adam_step(params, grads, m, v, step: int, lr: float, stream=None):
+    _check_f32(params, grads, m, v)
+    return _check(lib().mgx_mlp_adam_step(_ptr(params), _ptr(grads), _ptr(m), _ptr(v), step, lr, _stream(stream)),
+                  "mgx_mlp_adam_step")

@@ -4,11 +4,11 @@
 // (1D-row-block/mulmat_kernel.cu:39-80 and 100-142): C = A*B, or C += (A*B summed over the chunk).
 //
 // Design (one CTA per SM, persistent):
-//   * warp 8 (producer): one lane issues TMA 2D tile loads of A (128 x 32 doubles, two 128-byte
-//     swizzled boxes) and B (32 x 128 doubles, eight boxes) into a 3-stage ring, each stage
-//     guarded by a full/empty mbarrier pair.  No multicast.
-//   * warps 0-7 (consumers): a 2 x 4 warp grid, each warp owning a 64 x 32 block of the
-//     128 x 128 output tile as 4 x 4 DMMA m16n8k4 accumulators (64 doubles per lane).
+//   * warpgroup 0 (producer, 40 registers): one lane of warp 0 issues TMA 2D tile loads of A
+//     (128 x 32 doubles, two 128-byte swizzled boxes) and B (32 x 128 doubles, eight boxes) into
+//     a 3-stage ring, each stage guarded by a full/empty mbarrier pair.  No multicast.
+//   * warpgroups 1-2 (consumers, 232 registers): a 2 x 4 warp grid, each warp owning a 64 x 32 block of the
+//     128 x 128 output tile as 4 x 4 DMMA m16n8k8 accumulators (64 doubles per lane).
 //   * The reduction index is permuted inside every group of 8 (physical order 0,1,4,5 | 2,3,6,7)
 //     identically for A and B, so each fragment load from the swizzled tiles hits every shared
 //     memory bank exactly twice (the minimum for 256 bytes).
@@ -25,7 +25,15 @@ namespace fp64 {
 constexpr int BM = 128, BN = 128, BK = 32;
 constexpr int STAGES = 3;
 constexpr int CWARPS = 8;
-constexpr int THREADS = (CWARPS + 1) * 32;
+constexpr int PRODUCER_WARPS = 4;                         // one warpgroup; its warp 0 issues the loads
+constexpr int THREADS = (CWARPS + PRODUCER_WARPS) * 32;   // 384 = 3 warpgroups
+// Register split (setmaxnreg): the block launches with 384 x 168 registers; the producer
+// warpgroup gives back down to 40 each and the two consumer warpgroups take 232 each:
+// 128 x 40 + 256 x 232 = 64512 = 384 x 168.  The host refuses to launch unless the compiled
+// kernel has exactly LAUNCH_REGS registers per thread, so the split always adds up.
+constexpr int LAUNCH_REGS = 168, PRODUCER_REGS = 40, CONSUMER_REGS = 232;
+static_assert(PRODUCER_WARPS * 32 * PRODUCER_REGS + CWARPS * 32 * CONSUMER_REGS == THREADS * LAUNCH_REGS,
+              "register split must equal the launch budget");
 constexpr int A_BOX_BYTES = 128 * 128;       // 128 rows x 16 doubles
 constexpr int B_BOX_BYTES = BK * 128;        // 32 rows x 16 doubles
 constexpr int A_STAGE_BYTES = 2 * A_BOX_BYTES;
@@ -90,7 +98,7 @@ __device__ __forceinline__ uint32_t sw128(int row, int col16)
     return row * 128 + ((((col16 >> 1) ^ (row & 7)) & 7) << 4) + ((col16 & 1) << 3);
 }
 
-template <bool USE_TMA>
+template <bool USE_TMA, bool PANELS>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
 {
@@ -110,7 +118,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         fence_barrier_init();
     }
-    if (USE_TMA && warp == CWARPS && lane == 0) {
+    if (USE_TMA && warp == 0 && lane == 0) {
         tma_prefetch_desc(&tmA);
         tma_prefetch_desc(&tmB);
     }
@@ -121,7 +129,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int tiles = p.tiles ? p.num_tiles : tiles_m * tiles_n;
     const int kblocks = (p.k_len + BK - 1) / BK;
 
-    if (warp == CWARPS) {
+    if (warp < PRODUCER_WARPS) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(PRODUCER_REGS));
+        if (warp != 0) return;
         // ------------------------------------------------------------ producer
         int stage = 0;
         uint32_t phase = 0;
@@ -189,8 +199,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 
     // ---------------------------------------------------------------- consumers
-    const int wm = warp >> 2;  // 0..1
-    const int wn = warp & 3;   // 0..3
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(CONSUMER_REGS));
+    const int cw = warp - PRODUCER_WARPS;
+    const int wm = cw >> 2;  // 0..1
+    const int wn = cw & 3;   // 0..3
     const int g = lane >> 2;
     const int t = lane & 3;
 
@@ -258,29 +270,34 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t sB = sA + A_STAGE_BYTES;
 #pragma unroll
             for (int kb8 = 0; kb8 < 4; ++kb8) {
+                // One m16n8k8 per (mt, nt): logical k t -> physical k (t&1) + 4(t>>1), logical t+4 ->
+                // the same plus 2, i.e. the permutation 0,1,4,5 | 2,3,6,7 of the group of 8.  B
+                // fragments are loaded once per group; A fragments one 16-row tile at a time.
+                double bf[4][2];
 #pragma unroll
                 for (int step = 0; step < 2; ++step) {
-                    const int phys = (t & 1) + ((t >> 1) << 2) + 2 * step;  // k within the group of 8
-                    const uint32_t a_chunk = (uint32_t)((((kb8 & 1) * 4 + (t >> 1) * 2 + step) ^ g) << 4);
-                    double a0[4], a1[4], b0[4];
-#pragma unroll
-                    for (int mt = 0; mt < 4; ++mt) {
-                        const uint32_t base = sA + (kb8 >> 1) * A_BOX_BYTES + a_chunk;
-                        a0[mt] = lds_f64(base + a_row_off[mt][0]);
-                        a1[mt] = lds_f64(base + a_row_off[mt][1]);
-                    }
+                    const int phys = (t & 1) + ((t >> 1) << 2) + 2 * step;
 #pragma unroll
                     for (int nt = 0; nt < 4; ++nt) {
                         const int j = wn * 2 + (nt >> 1);
                         const int krow = kb8 * 8 + phys;
                         const uint32_t off = (uint32_t)(j * B_BOX_BYTES + krow * 128 +
                                                         (((((nt & 1) * 4) + (g >> 1)) ^ phys) << 4) + ((g & 1) << 3));
-                        b0[nt] = lds_f64(sB + off);
+                        bf[nt][step] = lds_f64(sB + off);
                     }
+                }
+                const uint32_t abase = sA + (kb8 >> 1) * A_BOX_BYTES;
+                const uint32_t c0 = (uint32_t)((((kb8 & 1) * 4 + (t >> 1) * 2) ^ g) << 4);
+                const uint32_t c1 = (uint32_t)((((kb8 & 1) * 4 + (t >> 1) * 2 + 1) ^ g) << 4);
 #pragma unroll
-                    for (int mt = 0; mt < 4; ++mt)
+                for (int mt = 0; mt < 4; ++mt) {
+                    double af[4];
+                    af[0] = lds_f64(abase + c0 + a_row_off[mt][0]);
+                    af[1] = lds_f64(abase + c0 + a_row_off[mt][1]);
+                    af[2] = lds_f64(abase + c1 + a_row_off[mt][0]);
+                    af[3] = lds_f64(abase + c1 + a_row_off[mt][1]);
 #pragma unroll
-                        for (int nt = 0; nt < 4; ++nt) dmma_16x8x4(acc[mt][nt], a0[mt], a1[mt], b0[nt]);
+                    for (int nt = 0; nt < 4; ++nt) dmma_16x8x8(acc[mt][nt], af, bf[nt]);
                 }
             }
             __syncwarp();
@@ -289,7 +306,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 stage = 0;
                 phase ^= 1u;
             }
-            if (p.panel_kb > 0 && ((kb + 1) % p.panel_kb == 0) && kb + 1 < kblocks) {
+            if (PANELS && ((kb + 1) % p.panel_kb == 0) && kb + 1 < kblocks) {
                 // end of a SUMMA panel: C_ij += panel product, one rounding, as the reference
                 store_acc(acc, m0, n0, m_end, n_end, 1);
 #pragma unroll
@@ -301,7 +318,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
         if (!ok) return;
-        store_acc(acc, m0, n0, m_end, n_end, p.panel_kb > 0 ? 1 : p.beta_one);
+        store_acc(acc, m0, n0, m_end, n_end, PANELS ? 1 : p.beta_one);
     }
 }
 
@@ -365,15 +382,24 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
     const int total_tiles = tiles_list_or(tiles, num_tiles, m, n);
     int grid = mgx_sm_count();
     if (grid > total_tiles) grid = total_tiles;
-    if (use_tma) {
-        MGX_HOST_CHECK(cudaFuncSetAttribute(fp64::dgemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            fp64::SMEM_BYTES));
-        fp64::dgemm_kernel<true><<<grid, fp64::THREADS, fp64::SMEM_BYTES, stream>>>(tmA, tmB, p);
-    } else {
-        MGX_HOST_CHECK(cudaFuncSetAttribute(fp64::dgemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            fp64::SMEM_BYTES));
-        fp64::dgemm_kernel<false><<<grid, fp64::THREADS, fp64::SMEM_BYTES, stream>>>(tmA, tmB, p);
-    }
+    auto launch = [&](auto kernel) -> int {
+        cudaFuncAttributes fa;
+        MGX_HOST_CHECK(cudaFuncGetAttributes(&fa, kernel));
+        if (fa.numRegs != fp64::LAUNCH_REGS) {
+            mgx_set_last_message("FP64 kernel compiled with %d registers/thread, expected %d for its register split",
+                                 fa.numRegs, fp64::LAUNCH_REGS);
+            return MGX_E_UNSUPPORTED;
+        }
+        MGX_HOST_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, fp64::SMEM_BYTES));
+        kernel<<<grid, fp64::THREADS, fp64::SMEM_BYTES, stream>>>(tmA, tmB, p);
+        return MGX_SUCCESS;
+    };
+    int rc;
+    if (use_tma)
+        rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<true, true>) : launch(fp64::dgemm_kernel<true, false>);
+    else
+        rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<false, true>) : launch(fp64::dgemm_kernel<false, false>);
+    if (rc != MGX_SUCCESS) return rc;
     MGX_HOST_CHECK(cudaGetLastError());
     return MGX_SUCCESS;
 }

@@ -14,11 +14,13 @@
 // Kernels:
 //   ozaki_row_exp   row maxima of A (one warp per row)
 //   ozaki_col_max   column maxima of B (atomicMax on the bit pattern of |b|)
-//   ozaki_split_a   digits of A as [t][i][kp] int8 (K-major)
-//   ozaki_split_b   digits of B transposed to [u][j][kp] int8 (K-major) through shared memory
+//   ozaki_split_a   digits of A as swizzled K-major tiles, blocked [row tile][K block][slice]
+//   ozaki_split_b   digits of B^T in the same layout, transposed through shared memory
 //   ozaki_gemm      persistent tcgen05 kernel, one 128 x 128 output tile at a time:
-//       warp 0      TMA producer: for each 32-byte K block, the slices a weight set needs
-//                   (128 rows x 32 bytes each, 32-byte swizzle) into a 3-stage ring
+//       warp 0      producer: one bulk copy per operand and K block moves every slice a weight
+//                   set needs (already in the MMA's 32-byte-swizzled tile image), for
+//                   floor(s / slices) consecutive 32-byte K blocks per stage, so every stage
+//                   carries about 2s tiles, into a 3-stage ring
 //       warp 1      TMEM owner and MMA issuer: tcgen05.mma.kind::i8, M=128 N=128 K=32, one
 //                   int32 accumulator (128 TMEM columns) per weight group, four groups per set
 //       warps 2-9   epilogue: tcgen05.ld of each group, FP64 Horner update held in registers
@@ -53,8 +55,8 @@ struct GemmParams {
     int stages;
     const int *ea;            // row exponents of A
     const int *eb;            // column exponents of B
-    const int4 *tiles;        // optional work list (m0, n0, m_end, n_end); null -> regular tiling
-    int num_tiles;
+    const uint8_t *da;        // digit tiles of A: [m/128][kblocks][splits][128 x 32 B], swizzled
+    const uint8_t *db;        // digit tiles of B^T, same layout over n
     int beta_one;
     int vec_store;
     int *status;
@@ -159,80 +161,87 @@ __device__ __forceinline__ void digits(double v, int e, int8_t (&d)[S], int s)
     }
 }
 
-// Each thread: 8 consecutive k of one row.  da layout [t][row][kp].
-__global__ void ozaki_split_a(const double *__restrict__ A, int m, int k, int lda, int kp, int s,
-                              const int *__restrict__ ea, int8_t *__restrict__ da)
+// Digit tiles are stored exactly as the MMA reads them from shared memory: for every 128-row
+// tile and 32-byte K block, the s slices follow each other, each a 128 x 32-byte K-major tile
+// with the 32-byte swizzle (the 16-byte half of row r is flipped when bit 2 of r is set).  One
+// bulk copy then moves every slice a stage needs.  Byte (row r, k byte c) of slice t of tile
+// (tm, kb) sits at ((tm * kblocks + kb) * s + t) * 4096 + r * 32 + (c ^ (((r >> 2) & 1) << 4)).
+__device__ __forceinline__ size_t slab_offset(int tile, int kb, int kblocks, int s, int r, int c)
 {
-    const int groups = kp / 8;
-    const size_t total = (size_t)m * groups;
-    const size_t slice = (size_t)m * kp;
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int row = (int)(idx / groups);
-        const int k0 = (int)(idx % groups) * 8;
-        int e = ea[row];
+    return ((size_t)tile * kblocks + kb) * (size_t)s * SLICE_TILE_BYTES + (size_t)r * 32 + (c ^ (((r >> 2) & 1) << 4));
+}
+
+// One warp per (8-row group, K block): lane -> row (lane / 4), 8 consecutive k (lane % 4).
+// Rows up to the 128-row padding and k up to the 32 padding get zero digits.
+__global__ void __launch_bounds__(256) ozaki_split_a(const double *__restrict__ A, int m, int k, int lda, int mp,
+                                                     int kblocks, int s, const int *__restrict__ ea,
+                                                     uint8_t *__restrict__ da)
+{
+    const int lane = threadIdx.x & 31;
+    const long long wpb = blockDim.x >> 5;
+    const long long items = (long long)(mp / 8) * kblocks;
+    for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < items; it += (long long)gridDim.x * wpb) {
+        const int ro = (int)(it / kblocks), kb = (int)(it % kblocks);
+        const int row = ro * 8 + (lane >> 2), kq = lane & 3;
+        const int k0 = kb * 32 + kq * 8;
+        int e = (row < m) ? ea[row] : 0;
         if (e == NONFINITE_EXP) e = 0;
         unsigned long long packed[MAX_SPLITS];
 #pragma unroll
         for (int t = 0; t < MAX_SPLITS; ++t) packed[t] = 0;
-        const double *arow = A + (size_t)row * lda;
+        const double *arow = A + (size_t)(row < m ? row : 0) * lda;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int kk = k0 + j;
-            double v = (kk < k) ? __ldg(arow + kk) : 0.0;
+            double v = (row < m && kk < k) ? __ldg(arow + kk) : 0.0;
             if (!isfinite(v)) v = 0.0;
             int8_t dg[MAX_SPLITS];
             digits<MAX_SPLITS>(v, e, dg, s);
 #pragma unroll
             for (int t = 0; t < MAX_SPLITS; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
         }
-        for (int t = 0; t < s; ++t)
-            *reinterpret_cast<unsigned long long *>(da + t * slice + (size_t)row * kp + k0) = packed[t];
+        const size_t off = slab_offset(row >> 7, kb, kblocks, s, row & 127, kq * 8);
+#pragma unroll
+        for (int t = 0; t < MAX_SPLITS; ++t)
+            if (t < s) *reinterpret_cast<unsigned long long *>(da + off + (size_t)t * SLICE_TILE_BYTES) = packed[t];
     }
 }
 
-// Block: 64 k x 64 columns of B.  db layout [u][col][kp].
-__global__ void __launch_bounds__(256) ozaki_split_b(const double *__restrict__ B, int k, int n, int ldb, int kp,
-                                                     int s, const int *__restrict__ eb, int8_t *__restrict__ db)
+// Block: 32 k x 128 columns of B through shared memory (coalesced reads along the columns),
+// written as the digit tiles of B^T (column j of B is row j of the tile).
+__global__ void __launch_bounds__(256) ozaki_split_b(const double *__restrict__ B, int k, int n, int ldb, int kblocks,
+                                                     int s, const int *__restrict__ eb, uint8_t *__restrict__ db)
 {
-    __shared__ double tileB[64][65];
-    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
-    for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
-        const int r = idx / 64, c = idx % 64;
-        const int kk = k0 + r, jj = j0 + c;
-        double v = (kk < k && jj < n) ? __ldg(B + (size_t)kk * ldb + jj) : 0.0;
+    __shared__ double tb[32][129];
+    const int tn = blockIdx.x, kb = blockIdx.y;
+    const int n0 = tn * 128, k0 = kb * 32;
+    for (int idx = threadIdx.x; idx < 32 * 128; idx += 256) {
+        const int kk = idx >> 7, c = idx & 127;
+        double v = (k0 + kk < k && n0 + c < n) ? __ldg(B + (size_t)(k0 + kk) * ldb + n0 + c) : 0.0;
         if (!isfinite(v)) v = 0.0;
-        tileB[r][c] = v;
+        tb[kk][c] = v;
     }
     __syncthreads();
-    // thread -> (column c, 16 consecutive k)
-    const int c = threadIdx.x >> 2;
-    const int kq = (threadIdx.x & 3) * 16;
-    const int jj = j0 + c;
-    if (jj >= n) return;
-    int e = eb[jj];
-    if (e == NONFINITE_EXP) e = 0;
-    unsigned long long lo[MAX_SPLITS], hi[MAX_SPLITS];
 #pragma unroll
-    for (int t = 0; t < MAX_SPLITS; ++t) lo[t] = hi[t] = 0;
+    for (int half = 0; half < 2; ++half) {
+        const int item = threadIdx.x + 256 * half;
+        const int r = item >> 2, kq = item & 3;   // tile row r = column n0 + r of B
+        int e = (n0 + r < n) ? eb[n0 + r] : 0;
+        if (e == NONFINITE_EXP) e = 0;
+        unsigned long long packed[MAX_SPLITS];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        int8_t dg[MAX_SPLITS];
-        digits<MAX_SPLITS>(tileB[kq + j][c], e, dg, s);
+        for (int t = 0; t < MAX_SPLITS; ++t) packed[t] = 0;
 #pragma unroll
-        for (int t = 0; t < MAX_SPLITS; ++t) {
-            const unsigned long long bits = (unsigned long long)(uint8_t)dg[t] << (8 * (j & 7));
-            if (j < 8) lo[t] |= bits;
-            else hi[t] |= bits;
+        for (int j = 0; j < 8; ++j) {
+            int8_t dg[MAX_SPLITS];
+            digits<MAX_SPLITS>(tb[kq * 8 + j][r], e, dg, s);
+#pragma unroll
+            for (int t = 0; t < MAX_SPLITS; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
         }
-    }
-    const size_t slice = (size_t)n * kp;
-    const int kk = k0 + kq;
-    if (kk < kp) {
-        for (int t = 0; t < s; ++t) {
-            int8_t *dst = db + t * slice + (size_t)jj * kp + kk;
-            *reinterpret_cast<ulonglong2 *>(dst) = make_ulonglong2(lo[t], hi[t]);
-        }
+        const size_t off = slab_offset(tn, kb, kblocks, s, r, kq * 8);
+#pragma unroll
+        for (int t = 0; t < MAX_SPLITS; ++t)
+            if (t < s) *reinterpret_cast<unsigned long long *>(db + off + (size_t)t * SLICE_TILE_BYTES) = packed[t];
     }
 }
 
@@ -285,31 +294,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ void tile_of(const GemmParams &p, int w, int &m0, int &n0, int &m_end, int &n_end)
+__device__ __forceinline__ void tile_of(const GemmParams &p, int w, int &m0, int &n0)
 {
-    if (p.tiles) {
-        const int4 t = p.tiles[w];
-        m0 = t.x;
-        n0 = t.y;
-        m_end = t.z;
-        n_end = t.w;
-    } else {
-        const int tiles_n = (p.n + TILE - 1) / TILE;
-        // groups of 8 tile rows sweep the columns together so their A slices stay in L2
-        const int tiles_m = (p.m + TILE - 1) / TILE;
-        const int per_group = 8 * tiles_n;
-        const int g = w / per_group, r = w % per_group;
-        const int first = g * 8;
-        const int gsize = min(tiles_m - first, 8);
-        m0 = (first + r % gsize) * TILE;
-        n0 = (r / gsize) * TILE;
-        m_end = p.m;
-        n_end = p.n;
-    }
+    // groups of 8 tile rows sweep the columns together so their A slices stay in L2
+    const int tiles_n = (p.n + TILE - 1) / TILE;
+    const int tiles_m = (p.m + TILE - 1) / TILE;
+    const int per_group = 8 * tiles_n;
+    const int g = w / per_group, r = w % per_group;
+    const int first = g * 8;
+    const int gsize = min(tiles_m - first, 8);
+    m0 = (first + r % gsize) * TILE;
+    n0 = (r / gsize) * TILE;
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
-    ozaki_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p)
+__global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__ GemmParams p)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -322,7 +320,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int total = p.tiles ? p.num_tiles : ((p.m + TILE - 1) / TILE) * ((p.n + TILE - 1) / TILE);
+    const int total = ((p.m + TILE - 1) / TILE) * ((p.n + TILE - 1) / TILE);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < p.stages; ++s) {
@@ -340,10 +338,6 @@ __global__ void __launch_bounds__(THREADS, 1)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (warp == 0 && lane == 0) {
-        tma_prefetch_desc(&tmA);
-        tma_prefetch_desc(&tmB);
-    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -356,24 +350,30 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t phase = 0;
             int armed[4] = {-1, -1, -1, -1};
             bool ok = true;
+            const size_t slab = (size_t)p.splits * SLICE_TILE_BYTES;  // all slices of one 128-row tile, one K block
             for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
-                int m0, n0, m_end, n_end;
-                tile_of(p, w, m0, n0, m_end, n_end);
+                int m0, n0;
+                tile_of(p, w, m0, n0);
+                const uint8_t *ga = p.da + (size_t)(m0 / TILE) * p.kblocks * slab;
+                const uint8_t *gb = p.db + (size_t)(n0 / TILE) * p.kblocks * slab;
                 for (int si = 0; si < p.num_sets && ok; ++si) {
                     const int nsl = min(p.splits, p.set_dhi[si] - 1);
-                    const uint32_t bytes = (uint32_t)(2 * nsl * SLICE_TILE_BYTES);
-                    for (int kb = 0; kb < p.kblocks; ++kb) {
+                    const int kpack = p.splits / nsl;   // K blocks per stage: every stage ~2s tiles
+                    const uint32_t bytes = (uint32_t)(nsl * SLICE_TILE_BYTES);
+                    for (int kb0 = 0; kb0 < p.kblocks; kb0 += kpack) {
                         if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty)) {
                             ok = false;
                             break;
                         }
+                        const int nkb = min(kpack, p.kblocks - kb0);
                         unsigned char *sa = smem + stage * p.stage_bytes;
                         unsigned char *sb = sa + p.splits * SLICE_TILE_BYTES;
-                        mbar_arrive_expect_tx(&full[stage], bytes);
+                        mbar_arrive_expect_tx(&full[stage], 2u * (uint32_t)nkb * bytes);
                         armed[stage] = (int)phase;
-                        for (int t = 0; t < nsl; ++t) {
-                            tma_load_3d(sa + t * SLICE_TILE_BYTES, &tmA, kb * KBLK, m0, t, &full[stage]);
-                            tma_load_3d(sb + t * SLICE_TILE_BYTES, &tmB, kb * KBLK, n0, t, &full[stage]);
+                        for (int j = 0; j < nkb; ++j) {
+                            // slices 1..nsl of K block kb0+j are contiguous: one bulk copy per operand
+                            bulk_load(sa + j * bytes, ga + (size_t)(kb0 + j) * slab, bytes, &full[stage]);
+                            bulk_load(sb + j * bytes, gb + (size_t)(kb0 + j) * slab, bytes, &full[stage]);
                         }
                         if (++stage == p.stages) {
                             stage = 0;
@@ -402,23 +402,28 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     acc_phase ^= 1u;
                     tc_fence_after();
-                    for (int kb = 0; kb < p.kblocks; ++kb) {
+                    const int kpack = p.splits / nsl;
+                    for (int kb0 = 0; kb0 < p.kblocks; kb0 += kpack) {
                         if (!mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull)) {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
+                        const int nkb = min(kpack, p.kblocks - kb0);
                         const uint32_t sa = smem_base + stage * p.stage_bytes;
                         const uint32_t sb = sa + p.splits * SLICE_TILE_BYTES;
-                        uint32_t started = (kb > 0) ? 0xFu : 0u;
-                        for (int t = 1; t <= nsl; ++t) {
-                            const int ulo = max(1, dlo - t), uhi = min(nsl, dhi - t);
-                            const uint64_t adesc = sw32_desc(sa + (t - 1) * SLICE_TILE_BYTES);
-                            for (int u = ulo; u <= uhi; ++u) {
-                                const int slot = dhi - (t + u);
-                                const uint64_t bdesc = sw32_desc(sb + (u - 1) * SLICE_TILE_BYTES);
-                                tc_mma_i8(tmem_base + slot * TILE, adesc, bdesc, IDESC_S8_128x128, (started >> slot) & 1u);
-                                started |= 1u << slot;
+                        uint32_t started = (kb0 > 0) ? 0xFu : 0u;
+                        for (int j = 0; j < nkb; ++j) {
+                            for (int t = 1; t <= nsl; ++t) {
+                                const int ulo = max(1, dlo - t), uhi = min(nsl, dhi - t);
+                                const uint64_t adesc = sw32_desc(sa + (j * nsl + t - 1) * SLICE_TILE_BYTES);
+                                for (int u = ulo; u <= uhi; ++u) {
+                                    const int slot = dhi - (t + u);
+                                    const uint64_t bdesc = sw32_desc(sb + (j * nsl + u - 1) * SLICE_TILE_BYTES);
+                                    tc_mma_i8(tmem_base + slot * TILE, adesc, bdesc, IDESC_S8_128x128,
+                                              (started >> slot) & 1u);
+                                    started |= 1u << slot;
+                                }
                             }
                         }
                         tc_commit(&empty[stage]);  // frees the stage once these MMAs have read it
@@ -441,8 +446,9 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint32_t acc_phase = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
-            int m0, n0, m_end, n_end;
-            tile_of(p, w, m0, n0, m_end, n_end);
+            int m0, n0;
+            tile_of(p, w, m0, n0);
+            const int m_end = p.m, n_end = p.n;
             double h[64];
 #pragma unroll
             for (int j = 0; j < 64; ++j) h[j] = 0.0;
@@ -527,26 +533,29 @@ namespace {
 
 struct WsLayout {
     size_t da, db, ea, eb, colmax, total;
-    int kp;
+    int kblocks;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 int ozaki_kmax(int s) { return (int)((2147483647ll / (4096ll * s)) & ~127ll); }
 
+// Workspace for one K range of at most ozaki_kmax(s): digit tiles of A (m rounded up to 128) and
+// of B^T (n rounded up to 128), each K block 32 bytes wide, then the exponents.
 WsLayout ws_layout(int m, int n, int k, int s)
 {
     WsLayout L;
     int kc = k;
     const int kmax = ozaki_kmax(s);
     if (kc > kmax) kc = kmax;
-    L.kp = (kc + 31) & ~31;
-    if (L.kp == 0) L.kp = 32;
+    L.kblocks = (kc + 31) / 32;
+    if (L.kblocks == 0) L.kblocks = 1;
+    const size_t mp = (size_t)((m + 127) / 128) * 128, np = (size_t)((n + 127) / 128) * 128;
     size_t off = 0;
     L.da = off;
-    off = align256(off + (size_t)s * m * L.kp);
+    off = align256(off + (size_t)s * mp * L.kblocks * 32);
     L.db = off;
-    off = align256(off + (size_t)s * n * L.kp);
+    off = align256(off + (size_t)s * np * L.kblocks * 32);
     L.ea = off;
     off = align256(off + sizeof(int) * (size_t)m);
     L.eb = off;
@@ -559,17 +568,18 @@ WsLayout ws_layout(int m, int n, int k, int s)
 
 }  // namespace
 
-// Phase 1: exponents and digit planes of A (m x k) and B (k x n) into the workspace (k <= kmax).
+// Phase 1: exponents and digit tiles of A (m x k) and B (k x n) into the workspace (k <= kmax).
 static int ozaki_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int s,
                             unsigned char *ws, const WsLayout &L, cudaStream_t stream)
 {
     int *status = mgx_device_status_ptr();
-    int8_t *da = reinterpret_cast<int8_t *>(ws + L.da);
-    int8_t *db = reinterpret_cast<int8_t *>(ws + L.db);
+    uint8_t *da = ws + L.da;
+    uint8_t *db = ws + L.db;
     int *ea = reinterpret_cast<int *>(ws + L.ea);
     int *eb = reinterpret_cast<int *>(ws + L.eb);
     unsigned long long *colmax = reinterpret_cast<unsigned long long *>(ws + L.colmax);
-    const int kp = (k + 31) & ~31;
+    const int kblocks = (k + 31) / 32;
+    const int mp = (m + 127) / 128 * 128, np = (n + 127) / 128 * 128;
     const int sms = mgx_sm_count();
 
     oz::ozaki_row_exp<<<(m + 7) / 8, 256, 0, stream>>>(A, m, k, lda, ea, status);
@@ -585,39 +595,27 @@ static int ozaki_split_impl(const double *A, const double *B, int m, int n, int 
         oz::ozaki_col_exp<<<(n + 255) / 256, 256, 0, stream>>>(colmax, n, eb, status);
         MGX_HOST_CHECK(cudaGetLastError());
     }
-    oz::ozaki_split_a<<<sms * 8, 256, 0, stream>>>(A, m, k, lda, kp, s, ea, da);
+    oz::ozaki_split_a<<<sms * 16, 256, 0, stream>>>(A, m, k, lda, mp, kblocks, s, ea, da);
     MGX_HOST_CHECK(cudaGetLastError());
     {
-        dim3 g((n + 63) / 64, (kp + 63) / 64);
-        oz::ozaki_split_b<<<g, 256, 0, stream>>>(B, k, n, ldb, kp, s, eb, db);
+        dim3 g(np / 128, kblocks);
+        oz::ozaki_split_b<<<g, 256, 0, stream>>>(B, k, n, ldb, kblocks, s, eb, db);
         MGX_HOST_CHECK(cudaGetLastError());
     }
     return MGX_SUCCESS;
 }
 
-// Phase 2: C (+)= recombined slice products (tcgen05 kernel); the work list is optional.
+// Phase 2: C (+)= recombined slice products (tcgen05 kernel).
 static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta_one, int s, const unsigned char *ws,
-                               const WsLayout &L, const int4 *tiles, int num_tiles, cudaStream_t stream)
+                               const WsLayout &L, cudaStream_t stream)
 {
-    const int kp = (k + 31) & ~31;
-    const int8_t *da = reinterpret_cast<const int8_t *>(ws + L.da);
-    const int8_t *db = reinterpret_cast<const int8_t *>(ws + L.db);
-    // tensor maps over the digit planes: dims {kp, rows, s}, box {32, 128, 1}, 32-byte swizzle
-    CUtensorMap tmA, tmB;
-    int rc = mgx_encode_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, da, (uint64_t)kp, (uint64_t)m, (uint64_t)s,
-                                (uint64_t)kp, (uint64_t)m * kp, oz::KBLK, oz::TILE, 1, CU_TENSOR_MAP_SWIZZLE_32B);
-    if (rc != MGX_SUCCESS) return rc;
-    rc = mgx_encode_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, db, (uint64_t)kp, (uint64_t)n, (uint64_t)s,
-                            (uint64_t)kp, (uint64_t)n * kp, oz::KBLK, oz::TILE, 1, CU_TENSOR_MAP_SWIZZLE_32B);
-    if (rc != MGX_SUCCESS) return rc;
-
     oz::GemmParams p;
     memset(&p, 0, sizeof p);
     p.C = C;
     p.m = m;
     p.n = n;
     p.ldc = ldc;
-    p.kblocks = kp / oz::KBLK;
+    p.kblocks = (k + 31) / 32;
     p.splits = s;
     // weight sets of up to four groups, highest weights first
     int d = s + 1, ns = 0;
@@ -638,18 +636,18 @@ static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta
     }
     p.ea = reinterpret_cast<const int *>(ws + L.ea);
     p.eb = reinterpret_cast<const int *>(ws + L.eb);
-    p.tiles = tiles;
-    p.num_tiles = num_tiles;
+    p.da = ws + L.da;
+    p.db = ws + L.db;
     p.beta_one = beta_one;
     p.vec_store = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
     p.status = mgx_device_status_ptr();
     const int smem = p.stages * p.stage_bytes + 1024 + 256;
     MGX_HOST_CHECK(cudaFuncSetAttribute(oz::ozaki_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int total = tiles ? num_tiles : ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE);
+    const int total = ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE);
     const int sms = mgx_sm_count();
     const int grid = sms < total ? sms : total;
     if (grid < 1) return MGX_SUCCESS;
-    oz::ozaki_gemm<<<grid, oz::THREADS, smem, stream>>>(tmA, tmB, p);
+    oz::ozaki_gemm<<<grid, oz::THREADS, smem, stream>>>(p);
     MGX_HOST_CHECK(cudaGetLastError());
     return MGX_SUCCESS;
 }
@@ -676,8 +674,7 @@ extern "C" MGX_API size_t mgx_ozaki_workspace_size(int m, int n, int k, int spli
 }
 
 int mgx_ozaki_run(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb, int ldc,
-                  int beta_one, int splits, void *workspace, size_t workspace_bytes, const int4 *tiles, int num_tiles,
-                  cudaStream_t stream)
+                  int beta_one, int splits, void *workspace, size_t workspace_bytes, cudaStream_t stream)
 {
     if (!ozaki_args_ok(m, n, k, splits) || (m > 0 && n > 0 && !C) ||
         (m > 0 && n > 0 && k > 0 && (!A || !B || lda < k || ldb < n)) || (m > 0 && n > 0 && ldc < n)) {
@@ -699,7 +696,7 @@ int mgx_ozaki_run(const double *A, const double *B, double *C, int m, int n, int
         unsigned char *ws = static_cast<unsigned char *>(workspace);
         int rc = ozaki_split_impl(A + k0, B + (size_t)k0 * ldb, m, n, kc, lda, ldb, splits, ws, L, stream);
         if (rc != MGX_SUCCESS) return rc;
-        rc = ozaki_multiply_impl(C, m, n, kc, ldc, (k0 > 0) ? 1 : beta_one, splits, ws, L, tiles, num_tiles, stream);
+        rc = ozaki_multiply_impl(C, m, n, kc, ldc, (k0 > 0) ? 1 : beta_one, splits, ws, L, stream);
         if (rc != MGX_SUCCESS) return rc;
     }
     return MGX_SUCCESS;
@@ -710,7 +707,7 @@ extern "C" MGX_API int mgx_gemm_ozaki(const double *A, const double *B, double *
                                       size_t workspace_bytes, void *stream)
 {
     return mgx_ozaki_run(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, splits, workspace, workspace_bytes,
-                         nullptr, 0, (cudaStream_t)stream);
+                         (cudaStream_t)stream);
 }
 
 // A-priori split choice.  The normwise error of the Ozaki form falls by close to two decimal
@@ -770,7 +767,7 @@ extern "C" MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ld
     const int wrc = ozaki_ws_check(const_cast<void *>(workspace), workspace_bytes, L, "mgx_ozaki_multiply");
     if (wrc != MGX_SUCCESS) return wrc;
     return ozaki_multiply_impl(C, m, n, k, ldc, beta_one ? 1 : 0, splits, static_cast<const unsigned char *>(workspace),
-                               L, nullptr, 0, (cudaStream_t)stream);
+                               L, (cudaStream_t)stream);
 }
 
 extern "C" MGX_API int mgx_ozaki_kmax(int splits)

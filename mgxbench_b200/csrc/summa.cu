@@ -5,8 +5,9 @@
 // its process column before C_ij += A_panel B_panel (mmb.cu:239-361).  Here A and B are resident,
 // so a plan turns the grid into a list of 128 x 128 work tiles clipped to their blocks, and one
 // persistent kernel walks (tile, panel) in order: the FP64 form adds each panel's product into
-// C_ij with one rounding, as the reference does; the Ozaki form accumulates the panels exactly in
-// int32 and recombines once.
+// C_ij with one rounding, as the reference does.  The Ozaki form accumulates the panels exactly
+// in int32 and recombines once; because its element values do not depend on how the output is
+// tiled, it covers every block with one uniform 128 x 128 raster of the whole C.
 #include <cstring>
 #include <vector>
 
@@ -16,8 +17,7 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
                         int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
                         const int4 *tiles, int num_tiles, int panel_kb);
 int mgx_ozaki_run(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb, int ldc,
-                  int beta_one, int splits, void *workspace, size_t workspace_bytes, const int4 *tiles, int num_tiles,
-                  cudaStream_t stream);
+                  int beta_one, int splits, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 struct mgx_summa_plan {
     mgx_summa_desc_t desc;
@@ -108,9 +108,8 @@ MGX_API int mgx_summa_run(mgx_summa_plan_t *P, const double *A, int lda, const d
     }
     const mgx_summa_desc_t &d = P->desc;
     cudaStream_t s = (cudaStream_t)stream;
-    if (d.form == MGX_FORM_OZAKI)
-        return mgx_ozaki_run(A, B, C, d.m, d.n, d.k, lda, ldb, ldc, 0, d.splits, P->ws, P->ws_bytes, P->d_tiles,
-                             P->num_tiles, s);
+    if (d.form == MGX_FORM_OZAKI)  // element values do not depend on the tiling: one uniform 128 x 128 raster
+        return mgx_ozaki_run(A, B, C, d.m, d.n, d.k, lda, ldb, ldc, 0, d.splits, P->ws, P->ws_bytes, s);
     // C = 0 (2D-block-matrix/mmb.cu:186), then every panel adds into it.
     MGX_HOST_CHECK(cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)d.n * sizeof(double), d.m, s));
     const int bk = d.panel_k < d.k ? d.panel_k : d.k;
