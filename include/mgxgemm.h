@@ -40,6 +40,9 @@ extern "C" {
 #define MGX_API
 #endif
 
+/* Arithmetic forms of the product. */
+typedef enum { MGX_FORM_FP64 = 0, MGX_FORM_OZAKI = 1 } mgx_form_t;
+
 typedef enum {
     MGX_SUCCESS = 0,
     MGX_E_INVALID = -1,      /* an argument is out of range (sizes, leading dimensions, null pointer) */
@@ -131,6 +134,17 @@ MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ldc, int beta
  * into chunks of this size and adds them in order). */
 MGX_API int mgx_ozaki_kmax(int splits);
 
+/* C = A B from HOST buffers (hA m x k, hB k x n, hC m x n, row-major, leading dimensions in
+ * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  B is copied and prepared once; then A is
+ * processed in `panels` row panels so that the host-to-device copy of the next panel, the
+ * products of this one and the device-to-host copy of the previous C panel overlap.  The
+ * result equals the device-buffer entry points'.  Device memory is taken stream-ordered from
+ * the current device's pool and returned before the call's work completes.  Page-locked host
+ * memory gives full copy/compute overlap.  Stream-ordered; the Ozaki form needs
+ * k <= mgx_ozaki_kmax(splits). */
+MGX_API int mgx_gemm_host(const double *hA, const double *hB, double *hC, int m, int n, int k, int lda, int ldb,
+                          int ldc, int form, int splits, int panels, void *stream);
+
 /* Split count the library picks to reach a normwise relative error <= target for inputs whose
  * per-row / per-column dynamic range is `exp_range` binades (a-priori model; 3..9). */
 MGX_API int mgx_ozaki_choose_splits(int k, double exp_range, double target);
@@ -146,8 +160,6 @@ MGX_API int mgx_ozaki_choose_splits(int k, double exp_range, double target);
  * be captured in a CUDA graph.  Blocks need not be equal (uneven splits, remainders).
  * ------------------------------------------------------------------------------------------ */
 
-typedef enum { MGX_FORM_FP64 = 0, MGX_FORM_OZAKI = 1 } mgx_form_t;
-
 typedef struct {
     int m, n, k;               /* C is m x n, the reduction is k */
     int grid_rows, grid_cols;  /* Pr x Pc process grid (2D-block-matrix/mmb.cu:45-58) */
@@ -160,6 +172,11 @@ typedef struct {
 } mgx_summa_desc_t;
 
 typedef struct mgx_summa_plan mgx_summa_plan_t;
+
+/* The FP64 plan's work list, computed on the host: returns the number of work tiles and writes up
+ * to `capacity` of them to out as {m0, n_lo, m_end, n_end} (columns [n_lo, n_end) of rows
+ * [m0, m_end)).  Needs no device. */
+MGX_API int mgx_summa_tiles(const mgx_summa_desc_t *desc, int *out, int capacity);
 
 /* Builds the work list on the current device and allocates the Ozaki workspace if needed. */
 MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t **plan);
@@ -228,6 +245,11 @@ MGX_API const char *mgx_status_string(int status);
 /* Measured peaks of this GPU's FP64 paths: kind 0 = DFMA on the FP64 units, 1 = DMMA m8n8k4,
  * 2 = DMMA m16n8k4, 3 = DMMA m16n8k8, 4 = DMMA m16n8k16.  Synchronous; writes TFLOP/s. */
 MGX_API int mgx_peak_fp64(int kind, int iterations, double *tflops_out);
+
+/* Measured INT8 tensor-core rate of tcgen05.mma.cta_group::1.kind::i8 with M = 128, K = 32 and
+ * N = 64 (kind 0), 128 (kind 1) or 256 (kind 2), operands resident in shared memory.
+ * Synchronous; writes TOP/s. */
+MGX_API int mgx_peak_int8(int kind, int iterations, double *tops_out);
 
 #ifdef __cplusplus
 }

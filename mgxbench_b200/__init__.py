@@ -67,6 +67,8 @@ EXPORTS = [
     ("mgx_ozaki_split", _i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_multiply", _i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_kmax", _i, [_i]),
+    ("mgx_gemm_host", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
+    ("mgx_summa_tiles", _i, [ctypes.POINTER(SummaDesc), ctypes.POINTER(_i), _i]),
     ("mgx_summa_plan_create", _i, [ctypes.POINTER(SummaDesc), ctypes.POINTER(_vp)]),
     ("mgx_summa_run", _i, [_vp, _vp, _i, _vp, _i, _vp, _i, _vp]),
     ("mgx_summa_plan_info", _i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_sz)]),
@@ -77,6 +79,7 @@ EXPORTS = [
     ("mgx_last_error_message", ctypes.c_char_p, []),
     ("mgx_status_string", ctypes.c_char_p, [_i]),
     ("mgx_peak_fp64", _i, [_i, _i, ctypes.POINTER(_d)]),
+    ("mgx_peak_int8", _i, [_i, _i, ctypes.POINTER(_d)]),
     ("mgx_mlp_param_count", _i, []),
     ("mgx_mlp_init", _i, [_vp, _u64, _vp]),
     ("mgx_mlp_forward", _i, [_vp, _i, _vp, _vp, _vp]),
@@ -218,12 +221,40 @@ def ozaki_multiply(C, k: int, splits: int, workspace, beta_one: bool = False, st
                                            workspace.numel(), _stream(stream)), "mgx_ozaki_multiply")
 
 
+def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=8, stream=None):
+    """C = A B from host (CPU, ideally pinned) float64 tensors, copies overlapped with compute."""
+    import torch
+    for t in (hA, hB, hC):
+        if t.dtype != torch.float64 or t.is_cuda or t.stride(-1) != 1:
+            raise MgxError(-1, "argument", "host matrices must be row-major float64 CPU tensors")
+    m, k = hA.shape
+    n = hB.shape[1]
+    return _check(lib().mgx_gemm_host(_ptr(hA), _ptr(hB), _ptr(hC), m, n, k, hA.stride(0), hB.stride(0),
+                                      hC.stride(0), form, splits, panels, _stream(stream)), "mgx_gemm_host")
+
+
 def ozaki_kmax(splits: int) -> int:
     return int(lib().mgx_ozaki_kmax(splits))
 
 
 def ozaki_choose_splits(k: int, exp_range: float, target: float = 1e-15) -> int:
     return int(lib().mgx_ozaki_choose_splits(k, exp_range, target))
+
+
+def summa_tiles(m, n, grid_rows, grid_cols, row_cuts=None, col_cuts=None):
+    """Host-side work list of a SUMMA plan: list of (m0, n_lo, m_end, n_end)."""
+    d = SummaDesc(m, n, 1, grid_rows, grid_cols, None, None, 1, FORM_FP64, 0)
+    keep = []
+    if row_cuts is not None:
+        keep.append((ctypes.c_int * len(row_cuts))(*row_cuts))
+        d.row_cuts = ctypes.cast(keep[-1], ctypes.POINTER(ctypes.c_int))
+    if col_cuts is not None:
+        keep.append((ctypes.c_int * len(col_cuts))(*col_cuts))
+        d.col_cuts = ctypes.cast(keep[-1], ctypes.POINTER(ctypes.c_int))
+    count = _check(lib().mgx_summa_tiles(ctypes.byref(d), None, 0), "mgx_summa_tiles")
+    buf = (ctypes.c_int * (4 * count))()
+    _check(lib().mgx_summa_tiles(ctypes.byref(d), buf, count), "mgx_summa_tiles")
+    return [tuple(buf[4 * i:4 * i + 4]) for i in range(count)]
 
 
 class SummaPlan:
@@ -289,6 +320,12 @@ def device_status() -> int:
     code = ctypes.c_int()
     _check(lib().mgx_device_status(ctypes.byref(code)), "mgx_device_status")
     return code.value
+
+
+def peak_int8(kind: int, iterations: int = 200000) -> float:
+    out = ctypes.c_double()
+    _check(lib().mgx_peak_int8(kind, iterations, ctypes.byref(out)), "mgx_peak_int8")
+    return out.value
 
 
 def peak_fp64(kind: int, iterations: int = 20000) -> float:

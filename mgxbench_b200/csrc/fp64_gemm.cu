@@ -13,8 +13,9 @@
 //     identically for A and B, so each fragment load from the swizzled tiles hits every shared
 //     memory bank exactly twice (the minimum for 256 bytes).
 //   * Epilogue: C = acc (beta 0) or C = C + acc (beta 1), one rounding, as the reference.
-// A variant whose producer warp loads with plain global loads handles layouts TMA cannot
-// describe (odd leading dimensions, misaligned pointers, odd K offsets).
+// Operands TMA cannot describe (odd leading dimension, odd K offset, unaligned base) are first
+// copied into stream-ordered scratch with an even pitch.  A variant whose producer warp loads
+// with plain global loads covers the one case with nothing to copy (a chunk wholly past k_total).
 #include <cstdio>
 
 #include "mgx_common.cuh"
@@ -62,13 +63,18 @@ struct Params {
 
 __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn);
 
+// Tile geometry.  n0 is where the tile's columns start in B and C; it is always even, because it
+// is the x coordinate of B's TMA boxes and TMA needs x * 8 bytes to be a multiple of 16.  A work
+// item may begin at an odd column n_lo (uneven SUMMA blocks): its tile then starts one column
+// earlier and the columns below n_lo, which belong to the neighbouring block, are not stored.
 __device__ __forceinline__ void tile_bounds(const Params &p, int tile, int tiles_m, int tiles_n, int &m0, int &n0,
-                                            int &m_end, int &n_end)
+                                            int &m_end, int &n_end, int &n_lo)
 {
     if (p.tiles) {
         const int4 t = p.tiles[tile];
         m0 = t.x;
-        n0 = t.y;
+        n_lo = t.y;
+        n0 = t.y & ~1;
         m_end = t.z;
         n_end = t.w;
     } else {
@@ -76,6 +82,7 @@ __device__ __forceinline__ void tile_bounds(const Params &p, int tile, int tiles
         tile_coords(tile, tiles_m, tiles_n, tm, tn);
         m0 = tm * BM;
         n0 = tn * BN;
+        n_lo = n0;
         m_end = p.m;
         n_end = p.n;
     }
@@ -139,8 +146,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int s = 0; s < STAGES; ++s) armed_parity[s] = -1;
         bool ok = true;
         for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-            int m0, n0, m_end, n_end;
-            tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end);
+            int m0, n0, m_end, n_end, n_lo;
+            tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
             for (int kb = 0; kb < kblocks; ++kb) {
                 bool got = true;
                 if (lane == 0) got = mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty);
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int h = 0; h < 2; ++h) a_row_off[mt][h] = (uint32_t)((wm * 64 + mt * 16 + h * 8 + g) * 128 + ((t & 1) << 3));
 
     // C (+)= acc for this lane's fragments, masked to the tile's bounds.
-    auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int beta_one) {
+    auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int n_lo, int beta_one) {
 #pragma unroll
         for (int mt = 0; mt < 4; ++mt) {
 #pragma unroll
@@ -228,7 +235,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int nt = 0; nt < 4; ++nt) {
                     const int col = n0 + wn * 32 + nt * 8 + 2 * t;
                     double v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-                    if (p.vec_store && col + 1 < n_end) {
+                    if (p.vec_store && col + 1 < n_end && col >= n_lo) {
                         double2 *dst = reinterpret_cast<double2 *>(crow + col);
                         if (beta_one) {
                             const double2 old = *dst;
@@ -237,8 +244,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                         }
                         *dst = make_double2(v0, v1);
                     } else {
-                        if (col < n_end) crow[col] = beta_one ? crow[col] + v0 : v0;
-                        if (col + 1 < n_end) crow[col + 1] = beta_one ? crow[col + 1] + v1 : v1;
+                        if (col < n_end && col >= n_lo) crow[col] = beta_one ? crow[col] + v0 : v0;
+                        if (col + 1 < n_end && col + 1 >= n_lo) crow[col + 1] = beta_one ? crow[col + 1] + v1 : v1;
                     }
                 }
             }
@@ -246,8 +253,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     };
 
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        int m0, n0, m_end, n_end;
-        tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end);
+        int m0, n0, m_end, n_end, n_lo;
+        tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
 
         double acc[4][4][4];
 #pragma unroll
@@ -308,7 +315,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             if (PANELS && ((kb + 1) % p.panel_kb == 0) && kb + 1 < kblocks) {
                 // end of a SUMMA panel: C_ij += panel product, one rounding, as the reference
-                store_acc(acc, m0, n0, m_end, n_end, 1);
+                store_acc(acc, m0, n0, m_end, n_end, n_lo, 1);
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -318,7 +325,19 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
         if (!ok) return;
-        store_acc(acc, m0, n0, m_end, n_end, PANELS ? 1 : p.beta_one);
+        store_acc(acc, m0, n0, m_end, n_end, n_lo, PANELS ? 1 : p.beta_one);
+    }
+}
+
+// dst[r][c] = src[r][col0 + c] for c < live, 0 for live <= c < cols, r < rows (rows >= src_rows
+// read as 0): an operand re-laid out with an even pitch and a 16-byte-aligned base for TMA.
+__global__ void pack_kernel(const double *__restrict__ src, int src_rows, int ld_src, int col0, int live,
+                            double *__restrict__ dst, int rows, int cols, int ld_dst)
+{
+    const size_t total = (size_t)rows * ld_dst;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / ld_dst), c = (int)(i % ld_dst);
+        dst[i] = (r < src_rows && c < live && c < cols) ? src[(size_t)r * ld_src + col0 + c] : 0.0;
     }
 }
 
@@ -365,9 +384,35 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
     p.num_tiles = num_tiles;
     p.panel_kb = panel_kb;
 
-    const bool tma_ok = !force_generic && ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
-                        ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (lda % 2 == 0) && (ldb % 2 == 0) &&
-                        (a_x0 % 2 == 0) && a_x_end > 0 && b_rows > 0;
+    const bool a_ok = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % 2 == 0) && (a_x0 % 2 == 0);
+    const bool b_ok = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % 2 == 0);
+    if (!force_generic && a_x_end > a_x0 && b_rows > 0 && (!a_ok || !b_ok)) {
+        // Re-lay the operands TMA cannot describe into stream-ordered scratch with an even pitch,
+        // then run the TMA kernel on the copies (an HBM-bound pass, small beside the product).
+        const int lda2 = (k_len + 1) & ~1, ldb2 = (n + 1) & ~1;
+        const size_t abytes = a_ok ? 0 : (size_t)m * lda2 * sizeof(double);
+        const size_t bbytes = b_ok ? 0 : (size_t)k_len * ldb2 * sizeof(double);
+        char *scratch = nullptr;
+        MGX_HOST_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&scratch), abytes + bbytes + 256, stream));
+        double *A2 = a_ok ? nullptr : reinterpret_cast<double *>(scratch);
+        double *B2 = b_ok ? nullptr : reinterpret_cast<double *>(scratch + ((abytes + 255) & ~size_t(255)));
+        const int blocks = mgx_sm_count() * 8;
+        if (A2) fp64::pack_kernel<<<blocks, 256, 0, stream>>>(A, m, lda, a_x0, a_x_end - a_x0, A2, m, k_len, lda2);
+        if (B2) fp64::pack_kernel<<<blocks, 256, 0, stream>>>(B, b_rows, ldb, 0, n, B2, k_len, n, ldb2);
+        int rc = MGX_SUCCESS;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            mgx_set_last_cuda_error(e, "operand packing", __FILE__, __LINE__);
+            rc = MGX_E_CUDA;
+        } else {
+            rc = mgx_launch_dgemm_ex(A2 ? A2 : A, B2 ? B2 : B, C, m, n, k_len, A2 ? 0 : a_x0, A2 ? k_len : a_x_end,
+                                     B2 ? k_len : b_rows, A2 ? lda2 : lda, B2 ? ldb2 : ldb, ldc, beta_one, stream, 0,
+                                     tiles, num_tiles, panel_kb);
+        }
+        cudaFreeAsync(scratch, stream);
+        return rc;
+    }
+    const bool tma_ok = !force_generic && a_ok && b_ok && a_x_end > 0 && b_rows > 0;
     CUtensorMap tmA, tmB;
     memset(&tmA, 0, sizeof tmA);
     memset(&tmB, 0, sizeof tmB);

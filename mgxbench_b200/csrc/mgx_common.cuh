@@ -121,6 +121,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     }
 }
 
+// Bounded wait for waits expected to be long (a warp idling through a whole phase of another
+// role's work): polls with a growing nanosleep so the waiting warp leaves the issue slots to
+// the warps doing the work.
+__device__ __forceinline__ bool mbar_wait_sleepy(uint64_t *bar, uint32_t parity, int *status, int code)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    unsigned ns = 64;
+    while (true) {
+        __nanosleep(ns);
+        if (mbar_try_wait(bar, parity)) return true;
+        if (ns < 2048) ns <<= 1;
+        if (global_ns() - t0 > kWaitLimitNs) {
+            record_status(status, code);
+            return false;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- TMA (no multicast anywhere)
 __device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar)
 {
@@ -148,6 +167,12 @@ __device__ __forceinline__ void bulk_load(void *smem_dst, const void *gsrc, uint
                      smem_u32(smem_dst)),
                  "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+// Asks L2 to fetch [gsrc, gsrc + bytes) ahead of use (no completion signal).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *gsrc, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map)

@@ -40,6 +40,7 @@ constexpr int SLICE_TILE_BYTES = TILE * KBLK;  // 4 KiB
 constexpr int MAX_SPLITS = 12;
 constexpr int MAX_SETS = 3;            // ceil(12 / 4): up to four weight groups (4 x 128 TMEM columns) per set
 constexpr int EPI_WARPS = 8;
+constexpr int PREFETCH_STAGES = 4;     // how far ahead the producer warms L2 with slabs
 constexpr int THREADS = (2 + EPI_WARPS) * 32;
 constexpr int NONFINITE_EXP = 0x7fffffff;
 
@@ -375,6 +376,12 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
                             bulk_load(sa + j * bytes, ga + (size_t)(kb0 + j) * slab, bytes, &full[stage]);
                             bulk_load(sb + j * bytes, gb + (size_t)(kb0 + j) * slab, bytes, &full[stage]);
                         }
+                        // warm L2 with the slabs this CTA will copy PREFETCH_STAGES stages from now
+                        const int kbp = kb0 + PREFETCH_STAGES * kpack;
+                        for (int j = 0; j < kpack && kbp + j < p.kblocks; ++j) {
+                            bulk_prefetch_l2(ga + (size_t)(kbp + j) * slab, bytes);
+                            bulk_prefetch_l2(gb + (size_t)(kbp + j) * slab, bytes);
+                        }
                         if (++stage == p.stages) {
                             stage = 0;
                             phase ^= 1u;
@@ -410,16 +417,17 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
                         }
                         tc_fence_after();
                         const int nkb = min(kpack, p.kblocks - kb0);
-                        const uint32_t sa = smem_base + stage * p.stage_bytes;
-                        const uint32_t sb = sa + p.splits * SLICE_TILE_BYTES;
+                        // descriptors of tile i of this stage differ only in the start-address field
+                        const uint64_t a0 = sw32_desc(smem_base + stage * p.stage_bytes);
+                        const uint64_t b0 = sw32_desc(smem_base + stage * p.stage_bytes + p.splits * SLICE_TILE_BYTES);
                         uint32_t started = (kb0 > 0) ? 0xFu : 0u;
                         for (int j = 0; j < nkb; ++j) {
                             for (int t = 1; t <= nsl; ++t) {
                                 const int ulo = max(1, dlo - t), uhi = min(nsl, dhi - t);
-                                const uint64_t adesc = sw32_desc(sa + (j * nsl + t - 1) * SLICE_TILE_BYTES);
+                                const uint64_t adesc = a0 + (uint64_t)((j * nsl + t - 1) * (SLICE_TILE_BYTES >> 4));
                                 for (int u = ulo; u <= uhi; ++u) {
                                     const int slot = dhi - (t + u);
-                                    const uint64_t bdesc = sw32_desc(sb + (j * nsl + u - 1) * SLICE_TILE_BYTES);
+                                    const uint64_t bdesc = b0 + (uint64_t)((j * nsl + u - 1) * (SLICE_TILE_BYTES >> 4));
                                     tc_mma_i8(tmem_base + slot * TILE, adesc, bdesc, IDESC_S8_128x128,
                                               (started >> slot) & 1u);
                                     started |= 1u << slot;
@@ -454,7 +462,7 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
             for (int j = 0; j < 64; ++j) h[j] = 0.0;
             for (int si = 0; si < p.num_sets; ++si) {
                 bool got = true;
-                if (lane == 0) got = mbar_wait_bounded(acc_full, acc_phase, p.status, kDevTimeoutAcc);
+                if (lane == 0) got = mbar_wait_sleepy(acc_full, acc_phase, p.status, kDevTimeoutAcc);
                 got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
                 if (!got) {
                     ok = false;
@@ -569,40 +577,48 @@ WsLayout ws_layout(int m, int n, int k, int s)
 }  // namespace
 
 // Phase 1: exponents and digit tiles of A (m x k) and B (k x n) into the workspace (k <= kmax).
-static int ozaki_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int s,
-                            unsigned char *ws, const WsLayout &L, cudaStream_t stream)
+static int ozaki_split_a_impl(const double *A, int m, int k, int lda, int s, unsigned char *ws, const WsLayout &L,
+                              cudaStream_t stream)
 {
     int *status = mgx_device_status_ptr();
-    uint8_t *da = ws + L.da;
-    uint8_t *db = ws + L.db;
     int *ea = reinterpret_cast<int *>(ws + L.ea);
+    const int kblocks = (k + 31) / 32;
+    const int mp = (m + 127) / 128 * 128;
+    oz::ozaki_row_exp<<<(m + 7) / 8, 256, 0, stream>>>(A, m, k, lda, ea, status);
+    MGX_HOST_CHECK(cudaGetLastError());
+    oz::ozaki_split_a<<<mgx_sm_count() * 16, 256, 0, stream>>>(A, m, k, lda, mp, kblocks, s, ea, ws + L.da);
+    MGX_HOST_CHECK(cudaGetLastError());
+    return MGX_SUCCESS;
+}
+
+static int ozaki_split_b_impl(const double *B, int n, int k, int ldb, int s, unsigned char *ws, const WsLayout &L,
+                              cudaStream_t stream)
+{
+    int *status = mgx_device_status_ptr();
     int *eb = reinterpret_cast<int *>(ws + L.eb);
     unsigned long long *colmax = reinterpret_cast<unsigned long long *>(ws + L.colmax);
     const int kblocks = (k + 31) / 32;
-    const int mp = (m + 127) / 128 * 128, np = (n + 127) / 128 * 128;
+    const int np = (n + 127) / 128 * 128;
     const int sms = mgx_sm_count();
-
-    oz::ozaki_row_exp<<<(m + 7) / 8, 256, 0, stream>>>(A, m, k, lda, ea, status);
-    MGX_HOST_CHECK(cudaGetLastError());
     MGX_HOST_CHECK(cudaMemsetAsync(colmax, 0, sizeof(unsigned long long) * (size_t)n, stream));
-    {
-        int ych = (sms * 8) / ((n + 255) / 256);
-        if (ych > (k + 63) / 64) ych = (k + 63) / 64;
-        if (ych < 1) ych = 1;
-        dim3 g((n + 255) / 256, ych);
-        oz::ozaki_col_max<<<g, 256, 0, stream>>>(B, k, n, ldb, colmax);
-        MGX_HOST_CHECK(cudaGetLastError());
-        oz::ozaki_col_exp<<<(n + 255) / 256, 256, 0, stream>>>(colmax, n, eb, status);
-        MGX_HOST_CHECK(cudaGetLastError());
-    }
-    oz::ozaki_split_a<<<sms * 16, 256, 0, stream>>>(A, m, k, lda, mp, kblocks, s, ea, da);
+    int ych = (sms * 8) / ((n + 255) / 256);
+    if (ych > (k + 63) / 64) ych = (k + 63) / 64;
+    if (ych < 1) ych = 1;
+    oz::ozaki_col_max<<<dim3((n + 255) / 256, ych), 256, 0, stream>>>(B, k, n, ldb, colmax);
     MGX_HOST_CHECK(cudaGetLastError());
-    {
-        dim3 g(np / 128, kblocks);
-        oz::ozaki_split_b<<<g, 256, 0, stream>>>(B, k, n, ldb, kblocks, s, eb, db);
-        MGX_HOST_CHECK(cudaGetLastError());
-    }
+    oz::ozaki_col_exp<<<(n + 255) / 256, 256, 0, stream>>>(colmax, n, eb, status);
+    MGX_HOST_CHECK(cudaGetLastError());
+    oz::ozaki_split_b<<<dim3(np / 128, kblocks), 256, 0, stream>>>(B, k, n, ldb, kblocks, s, eb, ws + L.db);
+    MGX_HOST_CHECK(cudaGetLastError());
     return MGX_SUCCESS;
+}
+
+static int ozaki_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int s,
+                            unsigned char *ws, const WsLayout &L, cudaStream_t stream)
+{
+    int rc = ozaki_split_a_impl(A, m, k, lda, s, ws, L, stream);
+    if (rc == MGX_SUCCESS) rc = ozaki_split_b_impl(B, n, k, ldb, s, ws, L, stream);
+    return rc;
 }
 
 // Phase 2: C (+)= recombined slice products (tcgen05 kernel).
@@ -774,4 +790,106 @@ extern "C" MGX_API int mgx_ozaki_kmax(int splits)
 {
     if (splits < 2 || splits > oz::MAX_SPLITS) return 0;
     return ozaki_kmax(splits);
+}
+
+// ------------------------------------------------------------------------------------------
+// Host-buffer entry point: PCIe copies overlapped with the product, row panel by row panel.
+// B goes to the device first and is sliced once; then for every panel of A rows the copy of
+// the next panel, the slicing and products of this one and the copy-back of the previous C
+// panel run on three streams.  The result is bit-identical to one mgx_gemm_ozaki call (the
+// exponents are per row of A and per column of B).
+int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
+                     int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic);
+
+extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double *hC, int m, int n, int k, int lda,
+                                     int ldb, int ldc, int form, int splits, int panels, void *stream)
+{
+    if (m < 0 || n < 0 || k < 0 || (m > 0 && n > 0 && (!hC || ldc < n)) ||
+        (m > 0 && n > 0 && k > 0 && (!hA || !hB || lda < k || ldb < n)) || (form != MGX_FORM_FP64 && form != MGX_FORM_OZAKI) ||
+        (form == MGX_FORM_OZAKI && (splits < 2 || splits > oz::MAX_SPLITS))) {
+        mgx_set_last_message("mgx_gemm_host: invalid arguments");
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0) return MGX_SUCCESS;
+    cudaStream_t s0 = (cudaStream_t)stream;
+    if (panels < 1) panels = 1;
+    if (panels > m) panels = m;
+    const bool ozaki = form == MGX_FORM_OZAKI && k > 0;
+    if (ozaki && k > ozaki_kmax(splits)) {
+        mgx_set_last_message("mgx_gemm_host: k = %d is above one int32 accumulation (%d) for %d splits", k,
+                             ozaki_kmax(splits), splits);
+        return MGX_E_UNSUPPORTED;
+    }
+    const int prow = (m + panels - 1) / panels;
+    const size_t kk = (size_t)(k > 0 ? k : 1);
+    const WsLayout L = ozaki ? ws_layout(prow, n, k, splits) : WsLayout{};
+    // device buffers: B, two A panels, two C panels, the Ozaki workspace
+    const size_t bB = align256(kk * n * sizeof(double)), bA = align256((size_t)prow * kk * sizeof(double)),
+                 bC = align256((size_t)prow * n * sizeof(double)), bW = ozaki ? L.total : 0;
+    char *mem = nullptr;
+    MGX_HOST_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&mem), bB + 2 * bA + 2 * bC + bW, s0));
+    double *dB = reinterpret_cast<double *>(mem);
+    double *dA[2] = {reinterpret_cast<double *>(mem + bB), reinterpret_cast<double *>(mem + bB + bA)};
+    double *dC[2] = {reinterpret_cast<double *>(mem + bB + 2 * bA), reinterpret_cast<double *>(mem + bB + 2 * bA + bC)};
+    unsigned char *ws = reinterpret_cast<unsigned char *>(mem + bB + 2 * bA + 2 * bC);
+
+    cudaStream_t sin = nullptr, sout = nullptr;
+    cudaEvent_t ev[8];
+    int rc = MGX_SUCCESS;
+    auto fail = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == MGX_SUCCESS) {
+            mgx_set_last_cuda_error(e, what, __FILE__, __LINE__);
+            rc = MGX_E_CUDA;
+        }
+    };
+    fail(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking), "stream");
+    fail(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < 8; ++i) fail(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming), "event");
+    // ev[0]: buffers allocated; ev[1,2]: A panel copied; ev[3,4]: C panel computed; ev[5,6]: C panel copied out
+    if (rc == MGX_SUCCESS) {
+        fail(cudaEventRecord(ev[0], s0), "record");
+        fail(cudaStreamWaitEvent(sin, ev[0], 0), "wait");
+        fail(cudaStreamWaitEvent(sout, ev[0], 0), "wait");
+        if (k > 0) fail(cudaMemcpy2DAsync(dB, n * sizeof(double), hB, (size_t)ldb * sizeof(double), n * sizeof(double), k,
+                                          cudaMemcpyHostToDevice, s0), "copy B");
+        if (ozaki && rc == MGX_SUCCESS) rc = ozaki_split_b_impl(dB, n, k, n, splits, ws, L, s0);
+    }
+    for (int p = 0; p < panels && rc == MGX_SUCCESS; ++p) {
+        const int r0 = p * prow, rows = (m - r0 < prow) ? m - r0 : prow;
+        if (rows <= 0) break;
+        const int b = p & 1;
+        if (p >= 2) fail(cudaStreamWaitEvent(sin, ev[3 + b], 0), "wait");      // dA[b] free once panel p-2 computed
+        if (k > 0)
+            fail(cudaMemcpy2DAsync(dA[b], kk * sizeof(double), hA + (size_t)r0 * lda, (size_t)lda * sizeof(double),
+                                   kk * sizeof(double), rows, cudaMemcpyHostToDevice, sin), "copy A panel");
+        fail(cudaEventRecord(ev[1 + b], sin), "record");
+        fail(cudaStreamWaitEvent(s0, ev[1 + b], 0), "wait");
+        if (p >= 2) fail(cudaStreamWaitEvent(s0, ev[5 + b], 0), "wait");      // dC[b] free once copied out
+        if (rc != MGX_SUCCESS) break;
+        if (ozaki) {
+            rc = ozaki_split_a_impl(dA[b], rows, k, (int)kk, splits, ws, L, s0);
+            if (rc == MGX_SUCCESS) rc = ozaki_multiply_impl(dC[b], rows, n, k, n, 0, splits, ws, L, s0);
+        } else {
+            rc = mgx_launch_dgemm(dA[b], dB, dC[b], rows, n, k, 0, k, k, (int)kk, n, n, 0, s0, 0);
+        }
+        fail(cudaEventRecord(ev[3 + b], s0), "record");
+        fail(cudaStreamWaitEvent(sout, ev[3 + b], 0), "wait");
+        fail(cudaMemcpy2DAsync(hC + (size_t)r0 * ldc, (size_t)ldc * sizeof(double), dC[b], n * sizeof(double),
+                               n * sizeof(double), rows, cudaMemcpyDeviceToHost, sout), "copy C panel");
+        fail(cudaEventRecord(ev[5 + b], sout), "record");
+    }
+    // join the side streams back into the caller's stream, then release the buffers
+    if (sout) {
+        cudaEventRecord(ev[7], sout);
+        cudaStreamWaitEvent(s0, ev[7], 0);
+    }
+    if (sin) {
+        cudaEventRecord(ev[0], sin);
+        cudaStreamWaitEvent(s0, ev[0], 0);
+    }
+    cudaFreeAsync(mem, s0);
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
+    if (sin) cudaStreamDestroy(sin);
+    if (sout) cudaStreamDestroy(sout);
+    return rc;
 }

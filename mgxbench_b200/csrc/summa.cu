@@ -45,7 +45,51 @@ static bool cuts_ok(const std::vector<int> &c, int extent)
     return true;
 }
 
+// Work tiles, block by block in rank order: {m0, n_lo, m_end, n_end}.  Rows start at the block's
+// first row.  Column tiles start at the block's first column rounded down to even (the kernel's
+// B boxes need an even column); n_lo keeps the block's exact first column so the kernel never
+// stores into the neighbouring block.
+static std::vector<int4> summa_tiles(const std::vector<int> &rcut, const std::vector<int> &ccut)
+{
+    std::vector<int4> tiles;
+    for (size_t bi = 0; bi + 1 < rcut.size(); ++bi)
+        for (size_t bj = 0; bj + 1 < ccut.size(); ++bj) {
+            const int c_lo = ccut[bj], c_hi = ccut[bj + 1], base = c_lo & ~1;
+            for (int r = rcut[bi]; r < rcut[bi + 1]; r += 128)
+                for (int c = base; c < c_hi; c += 128)
+                    tiles.push_back(make_int4(r, c < c_lo ? c_lo : c, rcut[bi + 1] < r + 128 ? rcut[bi + 1] : r + 128,
+                                              c_hi < c + 128 ? c_hi : c + 128));
+        }
+    return tiles;
+}
+
 extern "C" {
+
+MGX_API int mgx_summa_tiles(const mgx_summa_desc_t *desc, int *out, int capacity)
+{
+    if (!desc || desc->m <= 0 || desc->n <= 0 || desc->grid_rows <= 0 || desc->grid_cols <= 0 ||
+        desc->grid_rows > desc->m || desc->grid_cols > desc->n) {
+        mgx_set_last_message("mgx_summa_tiles: invalid descriptor");
+        return MGX_E_INVALID;
+    }
+    const std::vector<int> rc = desc->row_cuts ? std::vector<int>(desc->row_cuts, desc->row_cuts + desc->grid_rows + 1)
+                                               : even_cuts(desc->m, desc->grid_rows);
+    const std::vector<int> cc = desc->col_cuts ? std::vector<int>(desc->col_cuts, desc->col_cuts + desc->grid_cols + 1)
+                                               : even_cuts(desc->n, desc->grid_cols);
+    if (!cuts_ok(rc, desc->m) || !cuts_ok(cc, desc->n)) {
+        mgx_set_last_message("mgx_summa_tiles: block cuts must rise strictly from 0 to the extent");
+        return MGX_E_INVALID;
+    }
+    const std::vector<int4> t = summa_tiles(rc, cc);
+    if (out)
+        for (int i = 0; i < (int)t.size() && i < capacity; ++i) {
+            out[4 * i] = t[i].x;
+            out[4 * i + 1] = t[i].y;
+            out[4 * i + 2] = t[i].z;
+            out[4 * i + 3] = t[i].w;
+        }
+    return (int)t.size();
+}
 
 MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t **plan)
 {
@@ -69,14 +113,7 @@ MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t
         mgx_set_last_message("mgx_summa_plan_create: block cuts must rise strictly from 0 to the extent");
         return MGX_E_INVALID;
     }
-    // Work tiles: each block tiled from its own origin, block by block in rank order.
-    std::vector<int4> tiles;
-    for (int bi = 0; bi < desc->grid_rows; ++bi)
-        for (int bj = 0; bj < desc->grid_cols; ++bj)
-            for (int r = P->rcut[bi]; r < P->rcut[bi + 1]; r += 128)
-                for (int c = P->ccut[bj]; c < P->ccut[bj + 1]; c += 128)
-                    tiles.push_back(make_int4(r, c, P->rcut[bi + 1] < r + 128 ? P->rcut[bi + 1] : r + 128,
-                                              P->ccut[bj + 1] < c + 128 ? P->ccut[bj + 1] : c + 128));
+    std::vector<int4> tiles = summa_tiles(P->rcut, P->ccut);
     P->num_tiles = (int)tiles.size();
     cudaGetDevice(&P->device);
     if (cudaMalloc(&P->d_tiles, tiles.size() * sizeof(int4)) != cudaSuccess ||

@@ -41,3 +41,17 @@ def test_host_only_calls(mgx):
     assert L.mgx_ab_multiply(None, None, None, 4, 4, 4, 4, 4, 4, 0) == -1          # w must be positive
     assert L.mgx_gemm_fp64(None, None, None, -1, 4, 4, 4, 4, 4, 0, None) == -1
     assert L.mgx_gemm_ozaki(None, None, None, 4, 4, 4, 4, 4, 4, 0, 1, None, 0, None) == -1
+
+
+def test_summa_work_list_covers_blocks_once_with_even_tma_columns(mgx):
+    import numpy as np
+    for (m, n, pr, pc, rc, cc) in [(389, 613, 3, 5, None, None), (12288, 20480, 3, 5, None, None),
+                                   (300, 300, 2, 2, [0, 100, 300], [0, 251, 300]), (7, 9, 7, 9, None, None)]:
+        tiles = mgx.summa_tiles(m, n, pr, pc, rc, cc)
+        cover = np.zeros((m, n), np.int32)
+        for (m0, n_lo, m_end, n_end) in tiles:
+            assert m_end - m0 <= 128 and 0 < n_end - n_lo <= 128
+            assert (n_lo & ~1) + 128 >= n_end      # the tile's even TMA base reaches every stored column
+            cover[m0:m_end, n_lo:n_end] += 1
+        assert cover.min() == 1 and cover.max() == 1
+    assert len(mgx.summa_tiles(12288, 20480, 3, 5)) == 96 * 160

@@ -95,3 +95,24 @@ def test_ozaki_k_beyond_int32_headroom(mgx, oracle):
     dC = torch.empty((8, 8), dtype=torch.float64, device="cuda")
     mgx.gemm_ozaki(dev(A), dev(B), dC, splits=s)
     assert np.array_equal(bits(host(dC)), bits(oracle.ozaki_gemm(A, B, s)))
+
+
+@pytest.mark.parametrize("form,panels", [(1, 1), (1, 3), (0, 4)])
+def test_host_buffer_entry_point_matches_device_path(mgx, oracle, form, panels):
+    """mgx_gemm_host (PCIe copies overlapped with the product, row panel by row panel) gives the
+    same bits as the device-buffer entry points."""
+    import torch
+    rng = np.random.default_rng(11)
+    m, n, k = 333, 270, 515
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    hA = torch.from_numpy(A).pin_memory()
+    hB = torch.from_numpy(B).pin_memory()
+    hC = torch.full((m, n), np.nan, dtype=torch.float64).pin_memory()
+    mgx.gemm_host(hA, hB, hC, form=form, splits=8, panels=panels)
+    torch.cuda.synchronize()
+    dC = torch.empty((m, n), dtype=torch.float64, device="cuda")
+    if form == 1:
+        mgx.gemm_ozaki(dev(A), dev(B), dC, splits=8)
+    else:
+        mgx.gemm_fp64(dev(A), dev(B), dC)
+    assert np.array_equal(bits(hC.numpy()), bits(host(dC)))
