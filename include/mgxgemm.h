@@ -145,6 +145,20 @@ MGX_API int mgx_ozaki_kmax(int splits);
 MGX_API int mgx_gemm_host(const double *hA, const double *hB, double *hC, int m, int n, int k, int lda, int ldb,
                           int ldc, int form, int splits, int panels, void *stream);
 
+/* Size of the fixed workspace of mgx_gemm_ozaki_noalloc (32 MiB). */
+#define MGX_OZAKI_NOALLOC_BYTES (32u << 20)
+
+/* mgx_gemm_ozaki for callers that cannot allocate device memory at call time (inside a stream
+ * capture that must not gain allocation nodes, under an allocator that owns the device memory,
+ * after a no-allocation start-up phase).  No counterpart in MGXBench.  It allocates nothing: its
+ * workspace is a fixed device array of MGX_OZAKI_NOALLOC_BYTES that every GPU loading the library
+ * holds until exit, so it takes only products whose mgx_ozaki_workspace_size fits (for example
+ * m = n = k = 1024 with 8 splits) and returns MGX_E_WORKSPACE otherwise.  The first call on a
+ * device looks up the array's device address and should come before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU race.  Stream-ordered. */
+MGX_API int mgx_gemm_ozaki_noalloc(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                   int ldb, int ldc, int beta_one, int splits, void *stream);
+
 /* Split count the library picks to reach a normwise relative error <= target for inputs whose
  * per-row / per-column dynamic range is `exp_range` binades (a-priori model; 3..9). */
 MGX_API int mgx_ozaki_choose_splits(int k, double exp_range, double target);

@@ -67,6 +67,7 @@ EXPORTS = [
     ("mgx_ozaki_split", _i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_multiply", _i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_kmax", _i, [_i]),
+    ("mgx_gemm_ozaki_noalloc", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
     ("mgx_gemm_host", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
     ("mgx_summa_tiles", _i, [ctypes.POINTER(SummaDesc), ctypes.POINTER(_i), _i]),
     ("mgx_summa_plan_create", _i, [ctypes.POINTER(SummaDesc), ctypes.POINTER(_vp)]),

@@ -28,6 +28,7 @@
 // All waits are bounded (mgx_common.cuh); TMEM is always released before the CTA exits.
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "mgx_common.cuh"
 
@@ -892,4 +893,67 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
     if (sin) cudaStreamDestroy(sin);
     if (sout) cudaStreamDestroy(sout);
     return rc;
+}
+
+// ------------------------------------------------------------------------------------------
+// Ozaki product with no device allocation.
+//
+// Some callers cannot allocate device memory when they call in:
+//   - code inside a CUDA stream capture that must not add allocation nodes to its graph;
+//   - applications whose own allocator already owns the device memory (an MPI or NVSHMEM
+//     symmetric heap, a framework's caching allocator);
+//   - services that forbid allocation after start-up (real-time loops).
+// For them this entry point uses a fixed workspace: the file-scope device array below,
+// MGX_OZAKI_NOALLOC_BYTES (32 MiB) long.  Every GPU that loads this library holds it until the
+// process exits.  Products whose workspace would not fit are rejected.
+static __device__ __align__(256) unsigned char g_ozaki_noalloc_ws[MGX_OZAKI_NOALLOC_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64];
+}  // namespace
+
+extern "C" MGX_API int mgx_gemm_ozaki_noalloc(const double *A, const double *B, double *C, int m, int n, int k,
+                                              int lda, int ldb, int ldc, int beta_one, int splits, void *stream)
+{
+    if (splits < 2 || splits > oz::MAX_SPLITS || m < 0 || n < 0 || k < 0) {
+        mgx_set_last_message("mgx_gemm_ozaki_noalloc: invalid arguments m=%d n=%d k=%d splits=%d", m, n, k, splits);
+        return MGX_E_INVALID;
+    }
+    const size_t need = ws_layout(m, n, k, splits).total;
+    if (need > (size_t)MGX_OZAKI_NOALLOC_BYTES) {
+        mgx_set_last_message("mgx_gemm_ozaki_noalloc: this product needs %zu bytes of workspace, more than the "
+                             "fixed %u-byte array; use mgx_gemm_ozaki with a caller-provided workspace",
+                             need, (unsigned)MGX_OZAKI_NOALLOC_BYTES);
+        return MGX_E_WORKSPACE;
+    }
+    // The array's name is a host-side stand-in; the kernels need its device address, taken once
+    // per device with that device current (the first call on a device, which should therefore
+    // come before any stream capture).
+    int dev = 0;
+    MGX_HOST_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        mgx_set_last_message("mgx_gemm_ozaki_noalloc: device %d out of range", dev);
+        return MGX_E_UNSUPPORTED;
+    }
+    void *ws = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_ozaki_noalloc_ws);
+            if (e != cudaSuccess || !p) {
+                mgx_set_last_cuda_error(e, "cudaGetSymbolAddress(g_ozaki_noalloc_ws)", __FILE__, __LINE__);
+                return MGX_E_CUDA;
+            }
+            g_noalloc_ptr[dev] = p;
+        }
+        ws = g_noalloc_ptr[dev];
+    }
+    // Calls share the array: two calls whose work overlaps on the GPU (different streams, no
+    // ordering between them) race on it.  Everything a call reads from the array it first writes
+    // (the column maxima are cleared by the split phase), so the previous call's contents do not
+    // matter.
+    return mgx_ozaki_run(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, splits, ws,
+                         (size_t)MGX_OZAKI_NOALLOC_BYTES, (cudaStream_t)stream);
 }
