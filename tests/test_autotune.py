@@ -1,0 +1,73 @@
+"""Autotuner host logic without a GPU: candidate space, the regression baseline (the method in the
+reference's autotuning/predictive.py spirit), the choice rule and the regret measure."""
+import math
+
+import numpy as np
+
+from mgxbench_b200 import autotune as at
+
+
+def synthetic_rows(shapes, seed=0):
+    """A toy machine: FP64 at 30 TF/s with error 1e-15 * sqrt(K/1e3); Ozaki s at 4.5 POPS / (s(s+1)/2)
+    plus a 1 GB/s-per-byte split cost, error 10^(-8 - 2(s-4)) for wide ranges."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for (m, n, k, er) in shapes:
+        f = 2.0 * m * n * k
+        for c in at.candidates():
+            if c.tile == at.TILE_FP64:
+                t, e = f / 30e12, 1e-15 * math.sqrt(k / 1e3)
+            else:
+                t = f * c.splits * (c.splits + 1) / 2 / 4.5e15 + 8.0 * (m * k + k * n) / 3e12
+                e = max(10.0 ** (-8 - 2 * (c.splits - 4)) * (1 if er > 8 else 0.1), 5e-17)
+            t *= math.exp(rng.normal(0, 0.03))
+            rows.append({"m": m, "n": n, "k": k, "exp_range": er, "tile": c.tile, "splits": c.splits,
+                         "seconds": t, "error": e})
+    return rows
+
+
+def test_candidates_and_features():
+    cs = at.candidates()
+    assert cs[0].tile == at.TILE_FP64 and cs[0].splits == 0
+    assert [c.splits for c in cs[1:]] == list(range(3, 10))
+    f = at.features(1024, 2048, 4096, 20, cs[3])
+    assert f[:3] == [10.0, 11.0, 12.0] and f[3:] == [20.0, 1.0, 5.0]
+
+
+def test_random_shapes_and_memory_bound():
+    shapes = at.random_shapes(500, seed=1)
+    dims = np.array([s[:3] for s in shapes])
+    assert dims.min() >= 256 and dims.max() <= 32768
+    assert all(0 <= s[3] <= 40 for s in shapes)
+    assert at.shape_fits(32768, 32768, 32768) and not at.shape_fits(65536, 65536, 32768)
+
+
+def test_regression_baseline_and_choice():
+    train = synthetic_rows(at.random_shapes(300, seed=2))
+    held = synthetic_rows(at.random_shapes(60, seed=3))
+    reg = at.RegressionModel().fit(train)
+    c = at.choose(reg, 8192, 8192, 8192, 20, 1e-15)
+    assert c.tile == at.TILE_OZAKI_128 and c.splits in (8, 9)
+    r = at.regret(reg, held, 1e-15)
+    assert r["shapes"] == 60 and r["mean_regret"] >= 0.0
+    # an oracle that knows the measurements has zero regret
+    class Perfect:
+        def predict(self, m, n, k, er, cands):
+            out = []
+            for cc in cands:
+                x = next(x for x in held if (x["m"], x["n"], x["k"], x["exp_range"], x["tile"], x["splits"]) ==
+                         (m, n, k, er, cc.tile, cc.splits))
+                out.append((x["seconds"], x["error"]))
+            return out
+    p = at.regret(Perfect(), held, 1e-15)
+    assert p["mean_regret"] == 0.0 and p["misses"] == 0
+
+
+def test_sweep_db_append_and_resume(tmp_path):
+    db = at.SweepDB(tmp_path / "s.jsonl")
+    rows = synthetic_rows([(256, 512, 1024, 3)])
+    db.add(rows[:3])
+    db2 = at.SweepDB(tmp_path / "s.jsonl")
+    assert len(db2.rows) == 3 and db2.has(256, 512, 1024, 3, at.candidates()[0])
+    assert not db2.has(256, 512, 1024, 3, at.candidates()[5])
+    assert len(db2.digest()) == 16
