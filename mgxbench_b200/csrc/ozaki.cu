@@ -309,6 +309,85 @@ __device__ __forceinline__ void tile_of(const GemmParams &p, int w, int &m0, int
     n0 = (r / gsize) * TILE;
 }
 
+// Weight sets of up to four consecutive groups, highest weights first (the same rule as the
+// host's, at compile time so the MMA issue sequence can be unrolled completely).
+__host__ __device__ constexpr int set_lo_of(int dhi) { return (dhi - 3 > 2) ? dhi - 3 : 2; }
+__host__ __device__ constexpr int set_hi(int S, int si)
+{
+    int d = S + 1;
+    for (int i = 0; i < si; ++i) d = set_lo_of(d) - 1;
+    return d;
+}
+__host__ __device__ constexpr int num_sets_of(int S)
+{
+    int d = S + 1, n = 0;
+    while (d >= 2) {
+        d = set_lo_of(d) - 1;
+        ++n;
+    }
+    return n;
+}
+__host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// Issues every MMA of one stage of weight set SI (NKB <= KPACK K blocks, slices 1..NSL of each
+// operand per K block, tiles laid out [K block][slice]).  All loop bounds are compile-time, so
+// each MMA costs a descriptor add and the instruction itself.  The first product into each
+// group's accumulator in the first K block overwrites it (accumulate flag 0).
+template <int S, int SI>
+__device__ __forceinline__ void issue_stage(uint32_t tmem_base, uint64_t a0, uint64_t b0, int nkb, bool first_kb)
+{
+    constexpr int DHI = set_hi(S, SI), DLO = set_lo_of(DHI), NSL = cmin(S, DHI - 1), KPACK = S / NSL;
+#pragma unroll
+    for (int j = 0; j < KPACK; ++j) {
+        if (j < nkb) {
+            const uint32_t fresh = (first_kb && j == 0) ? 1u : 0u;
+#pragma unroll
+            for (int t = 1; t <= NSL; ++t) {
+#pragma unroll
+                for (int u = 1; u <= NSL; ++u) {
+                    if (t + u >= DLO && t + u <= DHI) {
+                        const int slot = DHI - (t + u);
+                        const bool first_of_slot = (t == cmax(1, (t + u) - NSL));
+                        const uint32_t acc = (first_of_slot && fresh) ? 0u : 1u;
+                        tc_mma_i8(tmem_base + slot * TILE,
+                                  a0 + (uint64_t)((j * NSL + t - 1) * (SLICE_TILE_BYTES >> 4)),
+                                  b0 + (uint64_t)((j * NSL + u - 1) * (SLICE_TILE_BYTES >> 4)), IDESC_S8_128x128, acc);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Runs weight set SI of one tile on the MMA thread: waits for the epilogue to free the
+// accumulators, then walks the K blocks stage by stage.  Returns false if a wait ran out.
+template <int S, int SI>
+__device__ __forceinline__ bool mma_set(const GemmParams &p, uint32_t smem_base, uint32_t tmem_base, uint64_t *full,
+                                        uint64_t *empty, uint64_t *acc_full, uint64_t *acc_empty, int &stage,
+                                        uint32_t &phase, uint32_t &acc_phase)
+{
+    constexpr int DHI = set_hi(S, SI), NSL = cmin(S, DHI - 1), KPACK = S / NSL;
+    if (!mbar_wait_bounded(acc_empty, acc_phase ^ 1u, p.status, kDevTimeoutAcc)) return false;
+    acc_phase ^= 1u;
+    tc_fence_after();
+    for (int kb0 = 0; kb0 < p.kblocks; kb0 += KPACK) {
+        if (!mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull)) return false;
+        tc_fence_after();
+        const uint32_t sa = smem_base + stage * p.stage_bytes;
+        issue_stage<S, SI>(tmem_base, sw32_desc(sa), sw32_desc(sa + S * SLICE_TILE_BYTES), min(KPACK, p.kblocks - kb0),
+                           kb0 == 0);
+        tc_commit(&empty[stage]);  // frees the stage once these MMAs have read it
+        if (++stage == p.stages) {
+            stage = 0;
+            phase ^= 1u;
+        }
+    }
+    tc_commit(acc_full);
+    return true;
+}
+
+template <int S>
 __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__ GemmParams p)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -400,49 +479,15 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true;
             const uint32_t smem_base = smem_u32(smem);
+            constexpr int NS = num_sets_of(S);
             for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
-                for (int si = 0; si < p.num_sets && ok; ++si) {
-                    const int dhi = p.set_dhi[si], dlo = p.set_dlo[si];
-                    const int nsl = min(p.splits, dhi - 1);
-                    if (!mbar_wait_bounded(acc_empty, acc_phase ^ 1u, p.status, kDevTimeoutAcc)) {
-                        ok = false;
-                        break;
-                    }
-                    acc_phase ^= 1u;
-                    tc_fence_after();
-                    const int kpack = p.splits / nsl;
-                    for (int kb0 = 0; kb0 < p.kblocks; kb0 += kpack) {
-                        if (!mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        const int nkb = min(kpack, p.kblocks - kb0);
-                        // descriptors of tile i of this stage differ only in the start-address field
-                        const uint64_t a0 = sw32_desc(smem_base + stage * p.stage_bytes);
-                        const uint64_t b0 = sw32_desc(smem_base + stage * p.stage_bytes + p.splits * SLICE_TILE_BYTES);
-                        uint32_t started = (kb0 > 0) ? 0xFu : 0u;
-                        for (int j = 0; j < nkb; ++j) {
-                            for (int t = 1; t <= nsl; ++t) {
-                                const int ulo = max(1, dlo - t), uhi = min(nsl, dhi - t);
-                                const uint64_t adesc = a0 + (uint64_t)((j * nsl + t - 1) * (SLICE_TILE_BYTES >> 4));
-                                for (int u = ulo; u <= uhi; ++u) {
-                                    const int slot = dhi - (t + u);
-                                    const uint64_t bdesc = b0 + (uint64_t)((j * nsl + u - 1) * (SLICE_TILE_BYTES >> 4));
-                                    tc_mma_i8(tmem_base + slot * TILE, adesc, bdesc, IDESC_S8_128x128,
-                                              (started >> slot) & 1u);
-                                    started |= 1u << slot;
-                                }
-                            }
-                        }
-                        tc_commit(&empty[stage]);  // frees the stage once these MMAs have read it
-                        if (++stage == p.stages) {
-                            stage = 0;
-                            phase ^= 1u;
-                        }
-                    }
-                    if (ok) tc_commit(acc_full);
-                }
+                ok = mma_set<S, 0>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage, phase, acc_phase);
+                if (NS > 1 && ok)
+                    ok = mma_set<S, (NS > 1 ? 1 : 0)>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage,
+                                                      phase, acc_phase);
+                if (NS > 2 && ok)
+                    ok = mma_set<S, (NS > 2 ? 2 : 0)>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage,
+                                                      phase, acc_phase);
             }
             // Drain: all MMAs this thread issued have finished before TMEM is released.
             tc_commit(drain);
@@ -659,14 +704,32 @@ static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta
     p.vec_store = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
     p.status = mgx_device_status_ptr();
     const int smem = p.stages * p.stage_bytes + 1024 + 256;
-    MGX_HOST_CHECK(cudaFuncSetAttribute(oz::ozaki_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int total = ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE);
     const int sms = mgx_sm_count();
     const int grid = sms < total ? sms : total;
     if (grid < 1) return MGX_SUCCESS;
-    oz::ozaki_gemm<<<grid, oz::THREADS, smem, stream>>>(p);
-    MGX_HOST_CHECK(cudaGetLastError());
-    return MGX_SUCCESS;
+    auto launch = [&](auto kernel) -> int {
+        MGX_HOST_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kernel<<<grid, oz::THREADS, smem, stream>>>(p);
+        MGX_HOST_CHECK(cudaGetLastError());
+        return MGX_SUCCESS;
+    };
+    switch (s) {
+    case 2: return launch(oz::ozaki_gemm<2>);
+    case 3: return launch(oz::ozaki_gemm<3>);
+    case 4: return launch(oz::ozaki_gemm<4>);
+    case 5: return launch(oz::ozaki_gemm<5>);
+    case 6: return launch(oz::ozaki_gemm<6>);
+    case 7: return launch(oz::ozaki_gemm<7>);
+    case 8: return launch(oz::ozaki_gemm<8>);
+    case 9: return launch(oz::ozaki_gemm<9>);
+    case 10: return launch(oz::ozaki_gemm<10>);
+    case 11: return launch(oz::ozaki_gemm<11>);
+    case 12: return launch(oz::ozaki_gemm<12>);
+    default:
+        mgx_set_last_message("mgx_gemm_ozaki: %d splits is outside 2..12", s);
+        return MGX_E_INVALID;
+    }
 }
 
 static bool ozaki_args_ok(int m, int n, int k, int splits)
