@@ -37,9 +37,9 @@ N_DEFAULT = 16384
 EXP_RANGE = 20
 ERROR_GATE = 1e-15
 CHECK_ROWS = 256
-# DRAM bytes per ozaki_gemm launch at N = 16384, s = 8, from the ncu capture summarised in
-# profiles/ozaki_gemm_n16384.md (None until that capture exists).
-OZAKI_GEMM_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per ozaki_gemm launch at N = 16384, s = 8, from the one-pass ncu
+# capture at full size summarised in profiles/ozaki_gemm_n4096.md (167.53 GB + 2.16 GB).
+OZAKI_GEMM_TRAFFIC_BYTES = 169.69e9
 
 
 def env_rank():

@@ -1,0 +1,162 @@
+"""Measurements of the five workload configurations this library is specified on, one JSON line
+each (python -m mgxbench_b200.configs [cfg1 cfg2 cfg3 cfg4 cfg5]).
+
+  cfg1  FP64 N = 1024, uniform [-1, 1), one 1D block
+  cfg2  FP64 N = 8192, uniform, 1D row-block with 4 row panels of 2048 x 8192 run in sequence
+  cfg3  Ozaki N = 16384, u * 2^e (e in [-20, 20]), split count swept 3..9, native FP64 beside
+  cfg4  2D SUMMA M = 12288, N = 20480, K = 16384, 3 x 5 grid, panel width 512, FP64 and Ozaki
+        forms, each one persistent plan replayed from a CUDA graph
+  cfg5  learned cost model: regret against the exhaustive sweep (needs a sweep database and a
+        trained model, see mgxbench_b200.autotune)
+
+Times are CUDA events on the launching stream after warm-up; errors are against the GPU
+double-double product (all rows for cfg1, sampled rows otherwise).  Inputs are seeded synthetic
+matrices with the shapes and distributions of the configurations.
+"""
+from __future__ import annotations
+
+import json
+import sys
+
+import torch
+
+import mgxbench_b200 as mgx
+
+
+def _events():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _time(fn, reps=3, warm=1):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps * 1e-3
+
+
+def _mat(r, c, kind, seed, e_range=0):
+    x = torch.empty((r, c), dtype=torch.float64, device="cuda")
+    mgx.fill_matrix(x, kind, e_range=e_range, seed=seed)
+    return x
+
+
+def cfg1():
+    n = 1024
+    A, B, C = _mat(n, n, 1, 11), _mat(n, n, 1, 12), torch.empty((n, n), dtype=torch.float64, device="cuda")
+    t = _time(lambda: mgx.ab_multiply(A, B, C), reps=20)
+    e = mgx.error_vs_dd(A, B, C)
+    return {"config": "cfg1", "form": "fp64", "n": n, "tflops": 2 * n ** 3 / t / 1e12, "seconds": t,
+            "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "rows_checked": e["rows_checked"]}
+
+
+def cfg2():
+    n, panels = 8192, 4
+    mi = n // panels
+    A, B, C = _mat(n, n, 1, 21), _mat(n, n, 1, 22), torch.empty((n, n), dtype=torch.float64, device="cuda")
+
+    def run():
+        for r in range(panels):
+            mgx.gemm_fp64(A[r * mi:(r + 1) * mi], B, C[r * mi:(r + 1) * mi])
+    t = _time(run, reps=3)
+    peak = max(mgx.peak_fp64(k, 20000) for k in (3, 4))
+    e = mgx.error_vs_dd(A, B, C, row_start=n // 2 - 128, row_count=256)
+    tf = 2 * n ** 3 / t / 1e12
+    return {"config": "cfg2", "form": "fp64", "n": n, "row_panels": panels, "tflops": tf, "seconds": t,
+            "fp64_peak_tflops": peak, "frac_of_fp64_peak": tf / peak, "normwise_err": e["normwise"],
+            "max_rel_err": e["max_rel"], "rows_checked": e["rows_checked"]}
+
+
+def cfg3(splits=range(3, 10)):
+    n, er = 16384, 20
+    A, B, C = _mat(n, n, 2, 31, er), _mat(n, n, 2, 32, er), torch.empty((n, n), dtype=torch.float64, device="cuda")
+    rows = (n // 2 - 128, 256)
+    out = []
+    tn = _time(lambda: mgx.gemm_fp64(A, B, C), reps=2)
+    en = mgx.error_vs_dd(A, B, C, *rows)
+    out.append({"config": "cfg3", "form": "fp64", "n": n, "tflops": 2 * n ** 3 / tn / 1e12, "seconds": tn,
+                "normwise_err": en["normwise"], "max_rel_err": en["max_rel"]})
+    for s in splits:
+        ws = torch.empty(mgx.ozaki_workspace_size(n, n, n, s), dtype=torch.uint8, device="cuda")
+        t = _time(lambda: mgx.gemm_ozaki(A, B, C, splits=s, workspace=_Fixed(ws)), reps=2)
+        e = mgx.error_vs_dd(A, B, C, *rows)
+        out.append({"config": "cfg3", "form": "ozaki", "splits": s, "n": n, "effective_tflops": 2 * n ** 3 / t / 1e12,
+                    "seconds": t, "int8_tops": 2 * n ** 3 * s * (s + 1) / 2 / t / 1e12,
+                    "normwise_err": e["normwise"], "max_rel_err": e["max_rel"],
+                    "max_componentwise_err": e["max_componentwise"], "meets_1e-15": e["normwise"] <= 1e-15,
+                    "speedup_vs_fp64": tn / t})
+        del ws
+    return out
+
+
+class _Fixed:
+    def __init__(self, t):
+        self.t = t
+
+    def get(self, nbytes):
+        return self.t
+
+
+def cfg4(splits=None, model=None):
+    M, N, K, pr, pc, bk = 12288, 20480, 16384, 3, 5, 512
+    A, B = _mat(M, K, 1, 41), _mat(K, N, 1, 42)
+    C = torch.empty((M, N), dtype=torch.float64, device="cuda")
+    if splits is None:
+        splits = mgx.ozaki_choose_splits(K, 0.0, 1e-15)
+        if model is not None:
+            from mgxbench_b200 import autotune as at
+            c = at.choose(model, M, N, K, 0, 1e-15)
+            if c.tile != at.TILE_FP64:
+                splits = c.splits
+    out = []
+    for form, s in ((mgx.FORM_FP64, 0), (mgx.FORM_OZAKI, splits)):
+        plan = mgx.SummaPlan(M, N, K, pr, pc, bk, form=form, splits=max(s, 2))
+        stream = torch.cuda.Stream()
+        plan.run(A, B, C, stream=stream)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            plan.run(A, B, C, stream=stream)
+        t = _time(g.replay, reps=3)
+        e = mgx.error_vs_dd(A, B, C, row_start=M // 2 - 128, row_count=256)
+        info = plan.info()
+        out.append({"config": "cfg4", "form": "fp64" if form == mgx.FORM_FP64 else "ozaki", "splits": s or None,
+                    "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}", "panel_k": bk, "panels": info["panels"],
+                    "work_tiles": info["work_tiles"], "tflops": 2 * M * N * K / t / 1e12, "seconds": t,
+                    "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": True,
+                    "persistent_launches_per_product": 1})
+        del g
+        plan.close()
+    return out
+
+
+def cfg5(db_path, model_path, target=1e-15):
+    from mgxbench_b200 import autotune as at
+    db = at.SweepDB(db_path)
+    train = [r for r in db.rows if r.get("set") == "train"]
+    held = [r for r in db.rows if r.get("set") == "heldout"]
+    mlp = at.MlpModel.load(model_path)
+    return {"config": "cfg5", "train_rows": len(train), "heldout_rows": len(held),
+            "mlp": at.regret(mlp, held, target), "regression": at.regret(at.RegressionModel().fit(train), held, target)}
+
+
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    which = [a for a in argv if a.startswith("cfg")] or ["cfg1", "cfg2", "cfg3", "cfg4"]
+    for w in which:
+        if w == "cfg5":
+            res = cfg5(*[a for a in argv if not a.startswith("cfg")][:2])
+        else:
+            res = globals()[w]()
+        for r in (res if isinstance(res, list) else [res]):
+            print(json.dumps(r), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
