@@ -107,6 +107,17 @@ MGX_API int mgx_validate_matrix_c(const double *d_c, int rows, int cols, double 
 MGX_API int mgx_gemm_fp64(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
                           int ldc, int beta_one, void *stream);
 
+/* Split-K form for products with too few 128 x 128 output tiles to fill the GPU: the K range is
+ * cut into `ksplit` slices (at most one per 32-wide K block) computed by separate CTAs, and the
+ * slice products are summed into C in slice order (deterministic).  The rounding differs from
+ * mgx_gemm_fp64 by the slice sums.  No counterpart in MGXBench; the autotuner picks ksplit.
+ * `workspace` (256-byte aligned) holds mgx_fp64_splitk_workspace_size(m, n, k, ksplit) bytes;
+ * 0 bytes means ksplit resolved to one slice and the call is mgx_gemm_fp64. */
+MGX_API size_t mgx_fp64_splitk_workspace_size(int m, int n, int k, int ksplit);
+MGX_API int mgx_gemm_fp64_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                 int ldb, int ldc, int beta_one, int ksplit, void *workspace,
+                                 size_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------------------------------------
  * Ozaki-scheme FP64 GEMM on the INT8 tensor cores (tcgen05, exact int32 TMEM accumulation)
  * ------------------------------------------------------------------------------------------ */
@@ -135,13 +146,14 @@ MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ldc, int beta
 MGX_API int mgx_ozaki_kmax(int splits);
 
 /* C = A B from HOST buffers (hA m x k, hB k x n, hC m x n, row-major, leading dimensions in
- * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  B is copied and prepared once; then A is
- * processed in `panels` row panels so that the host-to-device copy of the next panel, the
- * products of this one and the device-to-host copy of the previous C panel overlap.  The
- * result equals the device-buffer entry points'.  Device memory is taken stream-ordered from
- * the current device's pool and returned before the call's work completes.  Page-locked host
- * memory gives full copy/compute overlap.  Stream-ordered; the Ozaki form needs
- * k <= mgx_ozaki_kmax(splits). */
+ * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  A is cut into `panels` row panels and B
+ * into `panels` column panels (multiples of 128); the panels are copied in the order A_0, B_0,
+ * A_1, B_1, ... and every block (i, j) is computed as soon as A_i and B_j are on the device, then
+ * copied back while the rest computes, so PCIe copies in both directions overlap the product.
+ * The result is bit-identical to the device-buffer entry points'.  Device memory (A, B, C and
+ * the Ozaki workspace) is taken stream-ordered from the library's pool on the current device
+ * and returned before the call's work completes.  Page-locked host memory gives full
+ * copy/compute overlap.  Stream-ordered; the Ozaki form needs k <= mgx_ozaki_kmax(splits). */
 MGX_API int mgx_gemm_host(const double *hA, const double *hB, double *hC, int m, int n, int k, int lda, int ldb,
                           int ldc, int form, int splits, int panels, void *stream);
 

@@ -61,6 +61,8 @@ EXPORTS = [
     ("mgx_ab_multiply_accumulate_async", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
     ("mgx_validate_matrix_c", _i, [_vp, _i, _i, _d, _d, _d, _i, _i, ctypes.POINTER(Validation)]),
     ("mgx_gemm_fp64", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp]),
+    ("mgx_fp64_splitk_workspace_size", _sz, [_i, _i, _i, _i]),
+    ("mgx_gemm_fp64_splitk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_ozaki", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_choose_splits", _i, [_i, _d, _d]),
@@ -166,10 +168,22 @@ def validate_matrix_c(d_c, rows, cols, expected, abs_tol=1e-9, rel_tol=1e-12, ra
 
 
 # ------------------------------------------------------------------ library forms
-def gemm_fp64(A, B, C, beta_one: bool = False, stream=None):
+def fp64_splitk_workspace_size(m, n, k, ksplit) -> int:
+    return int(lib().mgx_fp64_splitk_workspace_size(m, n, k, ksplit))
+
+
+def gemm_fp64(A, B, C, beta_one: bool = False, stream=None, ksplit: int = 1, workspace=None):
+    """C (+)= A B on the FP64 tensor cores; ksplit > 1 cuts K into slices computed by separate
+    CTAs (for products with few output tiles) and needs a workspace (grown on demand)."""
     _check_f64(A, B, C)
     m, k = A.shape
     n = B.shape[1]
+    if ksplit > 1:
+        need = fp64_splitk_workspace_size(m, n, k, ksplit)
+        ws = (workspace or _default_ws).get(need)
+        return _check(lib().mgx_gemm_fp64_splitk(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
+                                                 int(beta_one), ksplit, _ptr(ws), ws.numel(), _stream(stream)),
+                      "mgx_gemm_fp64_splitk")
     return _check(lib().mgx_gemm_fp64(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
                                       int(beta_one), _stream(stream)), "mgx_gemm_fp64")
 

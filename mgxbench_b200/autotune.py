@@ -29,8 +29,11 @@ from pathlib import Path
 
 import numpy as np
 
-TILE_FP64 = 0          # native FP64 kernel (DMMA), no splits
+TILE_FP64 = 0          # native FP64 kernel (DMMA), 128 x 128 output tiles over the whole K range
 TILE_OZAKI_128 = 1     # Ozaki INT8 kernel, 128 x 128 output tiles
+# native FP64 kernel, 128 x 128 output tiles, K cut into 2 / 4 / 8 / 16 slices (split-K)
+TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16 = 2, 3, 4, 5
+FP64_KSPLIT = {TILE_FP64: 1, TILE_FP64_K2: 2, TILE_FP64_K4: 4, TILE_FP64_K8: 8, TILE_FP64_K16: 16}
 SPLITS = tuple(range(3, 10))
 ERROR_FLOOR = 1e-17
 
@@ -41,12 +44,35 @@ class Candidate:
     splits: int
 
     @property
+    def is_fp64(self) -> bool:
+        return self.tile in FP64_KSPLIT
+
+    @property
+    def ksplit(self) -> int:
+        return FP64_KSPLIT.get(self.tile, 1)
+
+    @property
     def name(self) -> str:
-        return "fp64" if self.tile == TILE_FP64 else f"ozaki{self.splits}"
+        if self.is_fp64:
+            return "fp64" if self.ksplit == 1 else f"fp64k{self.ksplit}"
+        return f"ozaki{self.splits}"
 
 
-def candidates():
-    return [Candidate(TILE_FP64, 0)] + [Candidate(TILE_OZAKI_128, s) for s in SPLITS]
+SPLITK_WORKSPACE_LIMIT = 4 << 30   # bytes of split-K partial products a candidate may need
+
+
+def splitk_applies(m, n, k, ksplit):
+    """A split-K candidate is offered when every slice gets a 32-wide K block and the partial
+    products fit SPLITK_WORKSPACE_LIMIT (the executables apply the same rule)."""
+    return ksplit == 1 or ((k + 31) // 32 >= ksplit and ksplit * m * n * 8 <= SPLITK_WORKSPACE_LIMIT)
+
+
+def candidates(m=None, n=None, k=None):
+    """Every configuration, or those that apply to an m x n x k product."""
+    fp64 = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16)]
+    if m is not None:
+        fp64 = [c for c in fp64 if splitk_applies(m, n, k, c.ksplit)]
+    return fp64 + [Candidate(TILE_OZAKI_128, s) for s in SPLITS]
 
 
 def features(m, n, k, exp_range, cand: Candidate):
@@ -73,8 +99,8 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
     errors = {}
     for c in cands:
         def run():
-            if c.tile == TILE_FP64:
-                mgx.gemm_fp64(A, B, C)
+            if c.is_fp64:
+                mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws)
             else:
                 mgx.gemm_ozaki(A, B, C, splits=c.splits, workspace=ws)
         run()
@@ -86,7 +112,7 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
         e1.record()
         e1.synchronize()
         t = e0.elapsed_time(e1) / reps * 1e-3
-        key = c.splits  # results do not depend on the tile of a form
+        key = (c.ksplit, c.splits)  # Ozaki results do not depend on the tile; FP64 ones on the K slices
         if key not in errors:
             rows = min(check_rows, m)
             errors[key] = mgx.error_vs_dd(A, B, C, row_start=(m - rows) // 2, row_count=rows)["normwise"]
@@ -132,8 +158,9 @@ def random_shapes(count, seed, lo=256, hi=32768, rmax=40):
 
 
 def shape_fits(m, n, k, limit_bytes=60 * 2 ** 30):
-    """Keeps a measurement within a bounded share of device memory (A, B, C, 9-slice workspace)."""
-    return 8 * (m * k + k * n + m * n) + 9 * (m + n) * k < limit_bytes
+    """Keeps a measurement within a bounded share of device memory (A, B, C, the 9-slice Ozaki
+    workspace and at most SPLITK_WORKSPACE_LIMIT of split-K partial products)."""
+    return 8 * (m * k + k * n + m * n) + 9 * (m + n) * k + SPLITK_WORKSPACE_LIMIT < limit_bytes
 
 
 # ------------------------------------------------------------------ models
@@ -191,7 +218,7 @@ class MlpModel:
         self.xmean = self.xstd = self.ymean = self.ystd = None
         self.loss_history = []
 
-    def fit(self, rows, epochs=400, batch=256, lr=3e-3, seed=0):
+    def fit(self, rows, epochs=1000, batch=256, lr=3e-3, seed=0):
         import torch
         import mgxbench_b200 as mgx
         X = np.array([features(r["m"], r["n"], r["k"], r["exp_range"], Candidate(r["tile"], r["splits"]))
@@ -235,6 +262,7 @@ class MlpModel:
 
     def save(self, path, digest=""):
         meta = {"format": "mgx-mlp-v1", "layers": [6, 64, 64, 2], "activation": "tanh", "training_set": digest,
+                "candidates": [[c.tile, c.splits] for c in candidates()],
                 "xmean": self.xmean.tolist(), "xstd": self.xstd.tolist(), "ymean": self.ymean.tolist(),
                 "ystd": self.ystd.tolist(), "params": self.params.cpu().numpy().tolist(),
                 "loss_history": self.loss_history}
@@ -254,7 +282,7 @@ class MlpModel:
 
 def choose(model, m, n, k, exp_range, target, cands=None, margin=1.0):
     """Fastest candidate whose predicted error is <= target / margin (largest split count if none)."""
-    cands = cands or candidates()
+    cands = cands or candidates(m, n, k)
     pred = model.predict(m, n, k, exp_range, cands)
     ok = [(t, c) for (t, e), c in zip(pred, cands) if e * margin <= target]
     if ok:
@@ -288,17 +316,45 @@ def regret(model, sweep_rows, target, margin=1.0):
             "miss_rate": misses / max(1, len(regs))}
 
 
+def accuracy(model, sweep_rows):
+    """How well a model predicts what was measured: median and 90th percentile of |ln(t_pred /
+    t_meas)| and of |log10(err_pred / err_meas)| over every (shape, candidate) of a sweep."""
+    shapes = {}
+    for r in sweep_rows:
+        shapes.setdefault((r["m"], r["n"], r["k"], r["exp_range"]), []).append(r)
+    lt, le = [], []
+    for (m, n, k, er), rs in shapes.items():
+        pred = model.predict(m, n, k, er, [Candidate(r["tile"], r["splits"]) for r in rs])
+        for (t, e), r in zip(pred, rs):
+            lt.append(abs(math.log(t / r["seconds"])))
+            le.append(abs(math.log10(max(e, ERROR_FLOOR) / max(r["error"], ERROR_FLOOR))))
+    return {"runtime_abs_ln_median": float(np.median(lt)), "runtime_abs_ln_p90": float(np.quantile(lt, 0.9)),
+            "error_abs_log10_median": float(np.median(le)), "error_abs_log10_p90": float(np.quantile(le, 0.9))}
+
+
+TARGETS = (1e-15, 1e-13, 1e-11, 1e-9, 1e-7)
+
+
+def evaluate(model, sweep_rows, targets=TARGETS):
+    """Regret at each accuracy target (1e-15 first) and prediction accuracy on a sweep."""
+    out = {"regret": {f"{t:.0e}": regret(model, sweep_rows, t) for t in targets},
+           "accuracy": accuracy(model, sweep_rows)}
+    out["mean_regret_over_targets"] = float(np.mean([v["mean_regret"] for v in out["regret"].values()]))
+    out["misses_over_targets"] = int(sum(v["misses"] for v in out["regret"].values()))
+    return out
+
+
 def run_sweep(db_path, train_shapes=2000, heldout_shapes=500, seed=0, budget_s=None, log=print):
     """Measures the training set (one random candidate per shape) and the exhaustive held-out
     sweep (every candidate per shape), appending to the JSONL database as it goes."""
     db = SweepDB(db_path)
     rng = np.random.default_rng(seed)
-    cands = candidates()
     t0 = time.time()
     train = [s for s in random_shapes(train_shapes * 2, seed + 1) if shape_fits(*s[:3])][:train_shapes]
     held = [s for s in random_shapes(heldout_shapes * 2, seed + 2) if shape_fits(*s[:3])][:heldout_shapes]
     for i, (m, n, k, er) in enumerate(train):
-        c = cands[int(rng.integers(len(cands)))]
+        cs = candidates(m, n, k)
+        c = cs[int(rng.integers(len(cs)))]
         if not db.has(m, n, k, er, c):
             rows = measure(m, n, k, er, [c], seed=i)
             for r in rows:
@@ -308,7 +364,7 @@ def run_sweep(db_path, train_shapes=2000, heldout_shapes=500, seed=0, budget_s=N
             log(f"budget reached after {i + 1} training shapes")
             return db
     for i, (m, n, k, er) in enumerate(held):
-        todo = [c for c in cands if not db.has(m, n, k, er, c)]
+        todo = [c for c in candidates(m, n, k) if not db.has(m, n, k, er, c)]
         if todo:
             rows = measure(m, n, k, er, todo, seed=100000 + i)
             for r in rows:
@@ -340,11 +396,10 @@ def main(argv=None):
     tr = sub.add_parser("train")
     tr.add_argument("--db", required=True)
     tr.add_argument("--out", required=True)
-    tr.add_argument("--epochs", type=int, default=400)
+    tr.add_argument("--epochs", type=int, default=1000)
     ev = sub.add_parser("evaluate")
     ev.add_argument("--db", required=True)
     ev.add_argument("--model", required=True)
-    ev.add_argument("--target", type=float, default=1e-15)
     ch = sub.add_parser("choose")
     ch.add_argument("--model", required=True)
     ch.add_argument("m", type=int)
@@ -366,12 +421,13 @@ def main(argv=None):
         db = SweepDB(a.db)
         train = [r for r in db.rows if r.get("set") == "train"]
         held = [r for r in db.rows if r.get("set") == "heldout"]
-        out = {"mlp": regret(MlpModel.load(a.model), held, a.target),
-               "regression": regret(RegressionModel().fit(train), held, a.target)}
+        out = {"mlp": evaluate(MlpModel.load(a.model), held),
+               "regression": evaluate(RegressionModel().fit(train), held)}
         print(json.dumps(out, indent=1))
     elif a.cmd == "choose":
         c = choose(MlpModel.load(a.model), a.m, a.n, a.k, a.exp_range, a.target)
-        print(json.dumps({"form": "fp64" if c.tile == TILE_FP64 else "ozaki", "tile": c.tile, "splits": c.splits}))
+        print(json.dumps({"form": "fp64" if c.is_fp64 else "ozaki", "tile": c.tile, "ksplit": c.ksplit,
+                          "splits": c.splits}))
     return 0
 
 

@@ -110,8 +110,9 @@ def cfg4(splits=None, model=None):
         splits = mgx.ozaki_choose_splits(K, 0.0, 1e-15)
         if model is not None:
             from mgxbench_b200 import autotune as at
-            c = at.choose(model, M, N, K, 0, 1e-15)
-            if c.tile != at.TILE_FP64:
+            plan_cands = [c for c in at.candidates() if c.ksplit == 1]  # SUMMA panels are the K split
+            c = at.choose(model, M, N, K, 0, 1e-15, plan_cands)
+            if not c.is_fp64:
                 splits = c.splits
     out = []
     for form, s in ((mgx.FORM_FP64, 0), (mgx.FORM_OZAKI, splits)):

@@ -68,6 +68,45 @@ int mgx_sm_count()
     return g_sm_count[dev];
 }
 
+// The library's own stream-ordered memory pool on each device, for short-lived scratch (operand
+// packing, the host-buffer pipeline, validation accumulators).  It keeps up to 8 GiB across
+// synchronisations, so repeated calls reuse their scratch instead of mapping fresh memory each
+// time (a process's default pool returns everything at every synchronisation), and it leaves
+// the process's default pool settings alone.
+static cudaMemPool_t g_pool[kMaxDevices];
+
+int mgx_scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream)
+{
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices) return MGX_E_CUDA;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_pool[dev]) {
+            cudaMemPoolProps props;
+            memset(&props, 0, sizeof props);
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t pool = nullptr;
+            cudaError_t e = cudaMemPoolCreate(&pool, &props);
+            if (e != cudaSuccess) {
+                mgx_set_last_cuda_error(e, "cudaMemPoolCreate", __FILE__, __LINE__);
+                return MGX_E_CUDA;
+            }
+            uint64_t keep = 8ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            g_pool[dev] = pool;
+        }
+    }
+    const cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, g_pool[dev], stream);
+    if (e != cudaSuccess) {
+        mgx_set_last_cuda_error(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
+        return MGX_E_CUDA;
+    }
+    return MGX_SUCCESS;
+}
+
 static int get_encoder()
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -126,6 +165,11 @@ int mgx_encode_tmap_3d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_byt
 }
 
 // Defined in the kernels' translation units.
+size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit);
+int mgx_launch_dgemm_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                            int ldc, int beta_one, int ksplit, void *partial, size_t partial_bytes,
+                            cudaStream_t stream);
+
 int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                      int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic);
 int mgx_validate_impl(const double *d_c, size_t count, double expected, double abs_tol, double rel_tol,
@@ -186,6 +230,25 @@ MGX_API int mgx_gemm_fp64(const double *A, const double *B, double *C, int m, in
         return MGX_E_INVALID;
     }
     return mgx_launch_dgemm(A, B, C, m, n, k, 0, k, k, lda, ldb, ldc, beta_one ? 1 : 0, (cudaStream_t)stream, 0);
+}
+
+MGX_API size_t mgx_fp64_splitk_workspace_size(int m, int n, int k, int ksplit)
+{
+    if (m < 0 || n < 0 || k < 0) return 0;
+    return mgx_fp64_splitk_bytes(m, n, k, ksplit);
+}
+
+MGX_API int mgx_gemm_fp64_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                 int ldb, int ldc, int beta_one, int ksplit, void *workspace,
+                                 size_t workspace_bytes, void *stream)
+{
+    if (!dims_ok(m, n, k, lda, ldb, ldc) || ksplit < 1 || (m > 0 && n > 0 && (!C || (k > 0 && (!A || !B))))) {
+        mgx_set_last_message("mgx_gemm_fp64_splitk: invalid arguments m=%d n=%d k=%d lda=%d ldb=%d ldc=%d ksplit=%d",
+                             m, n, k, lda, ldb, ldc, ksplit);
+        return MGX_E_INVALID;
+    }
+    return mgx_launch_dgemm_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, ksplit, workspace,
+                                   workspace_bytes, (cudaStream_t)stream);
 }
 
 MGX_API int mgx_ab_multiply(double *a, double *b, double *c, int m, int n, int k, int lda, int ldb, int ldc, int w)

@@ -59,6 +59,11 @@ struct Params {
     const int4 *tiles;  // optional work list (m0, n0, m_end, n_end); null -> regular tiling of m x n
     int num_tiles;
     int panel_kb;       // > 0: add the accumulator into C after every panel_kb K blocks (SUMMA panels)
+    int ksplit;         // > 1: split-K -- work item w is (tile w / ksplit, K slice w % ksplit)
+    int kb_split;       // K blocks per slice
+    double *partial;    // split-K: slice s of the product goes to partial + s * partial_stride
+    int partial_ld;     // even, so the partial rows are 16-byte aligned
+    size_t partial_stride;
 };
 
 __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn);
@@ -99,6 +104,18 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
     tn = r / gsize;
 }
 
+// Work item w: its output tile and the K blocks [kb_begin, kb_end) it reduces over.
+__device__ __forceinline__ void item_bounds(const Params &p, int w, int tiles_m, int tiles_n, int kblocks, int &m0,
+                                            int &n0, int &m_end, int &n_end, int &n_lo, int &kb_begin, int &kb_end,
+                                            int &slice)
+{
+    const int tile = p.ksplit > 1 ? w / p.ksplit : w;
+    slice = p.ksplit > 1 ? w % p.ksplit : 0;
+    tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
+    kb_begin = slice * p.kb_split;
+    kb_end = min(kblocks, kb_begin + p.kb_split);
+}
+
 // Swizzled byte offset of element (row, col16) inside a box whose rows are 128 bytes.
 __device__ __forceinline__ uint32_t sw128(int row, int col16)
 {
@@ -135,6 +152,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int tiles_n = (p.n + BN - 1) / BN;
     const int tiles = p.tiles ? p.num_tiles : tiles_m * tiles_n;
     const int kblocks = (p.k_len + BK - 1) / BK;
+    const int items = tiles * (p.ksplit > 1 ? p.ksplit : 1);
 
     if (warp < PRODUCER_WARPS) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(PRODUCER_REGS));
@@ -145,10 +163,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         int armed_parity[STAGES];
         for (int s = 0; s < STAGES; ++s) armed_parity[s] = -1;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-            int m0, n0, m_end, n_end, n_lo;
-            tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
-            for (int kb = 0; kb < kblocks; ++kb) {
+        for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
+            int m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
+            item_bounds(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
+            for (int kb = kb_begin; kb < kb_end; ++kb) {
                 bool got = true;
                 if (lane == 0) got = mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty);
                 got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
@@ -222,20 +240,22 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int mt = 0; mt < 4; ++mt)
         for (int h = 0; h < 2; ++h) a_row_off[mt][h] = (uint32_t)((wm * 64 + mt * 16 + h * 8 + g) * 128 + ((t & 1) << 3));
 
-    // C (+)= acc for this lane's fragments, masked to the tile's bounds.
-    auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int n_lo, int beta_one) {
+    // dst (+)= acc for this lane's fragments, masked to the tile's bounds (dst = C, or a split-K
+    // slice of the partial products).
+    auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int n_lo, int beta_one,
+                         double *dst_base, int ld, int vec_store) {
 #pragma unroll
         for (int mt = 0; mt < 4; ++mt) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
                 if (row >= m_end) continue;
-                double *crow = p.C + (size_t)row * p.ldc;
+                double *crow = dst_base + (size_t)row * ld;
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt) {
                     const int col = n0 + wn * 32 + nt * 8 + 2 * t;
                     double v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-                    if (p.vec_store && col + 1 < n_end && col >= n_lo) {
+                    if (vec_store && col + 1 < n_end && col >= n_lo) {
                         double2 *dst = reinterpret_cast<double2 *>(crow + col);
                         if (beta_one) {
                             const double2 old = *dst;
@@ -252,9 +272,9 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     };
 
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        int m0, n0, m_end, n_end, n_lo;
-        tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
+    for (int w = blockIdx.x; w < items; w += gridDim.x) {
+        int m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
+        item_bounds(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
 
         double acc[4][4][4];
 #pragma unroll
@@ -265,7 +285,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 
         bool ok = true;
-        for (int kb = 0; kb < kblocks; ++kb) {
+        for (int kb = kb_begin; kb < kb_end; ++kb) {
             bool got = true;
             if (lane == 0) got = mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull);
             got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
@@ -315,7 +335,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             if (PANELS && ((kb + 1) % p.panel_kb == 0) && kb + 1 < kblocks) {
                 // end of a SUMMA panel: C_ij += panel product, one rounding, as the reference
-                store_acc(acc, m0, n0, m_end, n_end, n_lo, 1);
+                store_acc(acc, m0, n0, m_end, n_end, n_lo, 1, p.C, p.ldc, p.vec_store);
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -325,7 +345,26 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
         if (!ok) return;
-        store_acc(acc, m0, n0, m_end, n_end, n_lo, PANELS ? 1 : p.beta_one);
+        if (p.ksplit > 1)
+            store_acc(acc, m0, n0, m_end, n_end, n_lo, 0, p.partial + (size_t)slice * p.partial_stride, p.partial_ld, 1);
+        else
+            store_acc(acc, m0, n0, m_end, n_end, n_lo, PANELS ? 1 : p.beta_one, p.C, p.ldc, p.vec_store);
+    }
+}
+
+// Split-K epilogue: C = (beta ? C : 0) + slice 0 + slice 1 + ... in that fixed order, so the
+// result does not depend on which CTA finished first.
+__global__ void splitk_reduce(double *__restrict__ C, int ldc, int beta_one, const double *__restrict__ P, int ld,
+                              size_t stride, int slices, int m, int n)
+{
+    for (int row = blockIdx.x; row < m; row += gridDim.x) {
+        for (int col = threadIdx.x; col < n; col += blockDim.x) {
+            const size_t o = (size_t)row * ld + col;
+            double v = P[o];
+            for (int s = 1; s < slices; ++s) v += P[o + (size_t)s * stride];
+            double *c = C + (size_t)row * ldc + col;
+            *c = beta_one ? *c + v : v;
+        }
     }
 }
 
@@ -351,11 +390,54 @@ static int tiles_list_or(const int4 *tiles, int num_tiles, int m, int n)
     return tiles ? num_tiles : ((m + fp64::BM - 1) / fp64::BM) * ((n + fp64::BN - 1) / fp64::BN);
 }
 
+// Split-K geometry: K blocks per slice and the number of non-empty slices for `ksplit` asked.
+static void splitk_geometry(int k_len, int ksplit, int *kb_split, int *slices)
+{
+    const int kblocks = (k_len + fp64::BK - 1) / fp64::BK;
+    if (ksplit < 1) ksplit = 1;
+    if (ksplit > kblocks) ksplit = kblocks > 0 ? kblocks : 1;
+    *kb_split = (kblocks + ksplit - 1) / ksplit;
+    *slices = *kb_split > 0 ? (kblocks + *kb_split - 1) / *kb_split : 1;
+}
+
+size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit)
+{
+    int kbs, slices;
+    splitk_geometry(k, ksplit, &kbs, &slices);
+    if (slices <= 1 || m <= 0 || n <= 0) return 0;
+    return (size_t)slices * (size_t)m * (size_t)((n + 1) & ~1) * sizeof(double) + 256;
+}
+
+static int launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
+                        int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
+                        const int4 *tiles, int num_tiles, int panel_kb, int ksplit, void *partial,
+                        size_t partial_bytes);
+
 // Launch C (+)= A[:, a_x0 : a_x0 + k_len] * B[0 : k_len, :] with the library's FP64 kernel.
 // a_x_end: A columns at or beyond it read as zero; b_rows: rows of B that exist.
 int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                         int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
                         const int4 *tiles, int num_tiles, int panel_kb)
+{
+    return launch_dgemm(A, B, C, m, n, k_len, a_x0, a_x_end, b_rows, lda, ldb, ldc, beta_one, stream, force_generic,
+                        tiles, num_tiles, panel_kb, 1, nullptr, 0);
+}
+
+// Split-K form of the above (regular tiling only): the K range is cut into `ksplit` slices whose
+// products land in `partial` (mgx_fp64_splitk_bytes bytes, 256-byte aligned) and are summed
+// into C in slice order by a second kernel.
+int mgx_launch_dgemm_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                            int ldc, int beta_one, int ksplit, void *partial, size_t partial_bytes,
+                            cudaStream_t stream)
+{
+    return launch_dgemm(A, B, C, m, n, k, 0, k, k, lda, ldb, ldc, beta_one, stream, 0, nullptr, 0, 0, ksplit,
+                        partial, partial_bytes);
+}
+
+static int launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
+                        int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
+                        const int4 *tiles, int num_tiles, int panel_kb, int ksplit, void *partial,
+                        size_t partial_bytes)
 {
     if (m <= 0 || n <= 0) return MGX_SUCCESS;
     if (k_len <= 0) {
@@ -383,6 +465,22 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
     p.tiles = tiles;
     p.num_tiles = num_tiles;
     p.panel_kb = panel_kb;
+    int kb_split = 0, slices = 1;
+    splitk_geometry(k_len, (tiles || panel_kb > 0) ? 1 : ksplit, &kb_split, &slices);
+    p.ksplit = slices;
+    p.kb_split = kb_split;
+    p.partial = nullptr;
+    p.partial_ld = (n + 1) & ~1;
+    p.partial_stride = (size_t)m * (size_t)p.partial_ld;
+    if (slices > 1) {
+        const size_t need = (size_t)slices * p.partial_stride * sizeof(double);
+        if (!partial || partial_bytes < need || (reinterpret_cast<uintptr_t>(partial) & 255)) {
+            mgx_set_last_message("FP64 split-K: workspace of %zu bytes (aligned to 256) needed, %zu given", need,
+                                 partial_bytes);
+            return MGX_E_WORKSPACE;
+        }
+        p.partial = reinterpret_cast<double *>(partial);
+    }
 
     const bool a_ok = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % 2 == 0) && (a_x0 % 2 == 0);
     const bool b_ok = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % 2 == 0);
@@ -393,7 +491,10 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
         const size_t abytes = a_ok ? 0 : (size_t)m * lda2 * sizeof(double);
         const size_t bbytes = b_ok ? 0 : (size_t)k_len * ldb2 * sizeof(double);
         char *scratch = nullptr;
-        MGX_HOST_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&scratch), abytes + bbytes + 256, stream));
+        {
+            const int arc = mgx_scratch_alloc(reinterpret_cast<void **>(&scratch), abytes + bbytes + 256, stream);
+            if (arc != MGX_SUCCESS) return arc;
+        }
         double *A2 = a_ok ? nullptr : reinterpret_cast<double *>(scratch);
         double *B2 = b_ok ? nullptr : reinterpret_cast<double *>(scratch + ((abytes + 255) & ~size_t(255)));
         const int blocks = mgx_sm_count() * 8;
@@ -405,9 +506,9 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
             mgx_set_last_cuda_error(e, "operand packing", __FILE__, __LINE__);
             rc = MGX_E_CUDA;
         } else {
-            rc = mgx_launch_dgemm_ex(A2 ? A2 : A, B2 ? B2 : B, C, m, n, k_len, A2 ? 0 : a_x0, A2 ? k_len : a_x_end,
-                                     B2 ? k_len : b_rows, A2 ? lda2 : lda, B2 ? ldb2 : ldb, ldc, beta_one, stream, 0,
-                                     tiles, num_tiles, panel_kb);
+            rc = launch_dgemm(A2 ? A2 : A, B2 ? B2 : B, C, m, n, k_len, A2 ? 0 : a_x0, A2 ? k_len : a_x_end,
+                              B2 ? k_len : b_rows, A2 ? lda2 : lda, B2 ? ldb2 : ldb, ldc, beta_one, stream, 0, tiles,
+                              num_tiles, panel_kb, ksplit, partial, partial_bytes);
         }
         cudaFreeAsync(scratch, stream);
         return rc;
@@ -424,9 +525,9 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
                                           (uint64_t)ldb * 8, 16, fp64::BK, CU_TENSOR_MAP_SWIZZLE_128B);
         use_tma = (ea == MGX_SUCCESS && eb == MGX_SUCCESS);
     }
-    const int total_tiles = tiles_list_or(tiles, num_tiles, m, n);
+    const int total_items = tiles_list_or(tiles, num_tiles, m, n) * slices;
     int grid = mgx_sm_count();
-    if (grid > total_tiles) grid = total_tiles;
+    if (grid > total_items) grid = total_items;
     auto launch = [&](auto kernel) -> int {
         cudaFuncAttributes fa;
         MGX_HOST_CHECK(cudaFuncGetAttributes(&fa, kernel));
@@ -446,6 +547,13 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
         rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<false, true>) : launch(fp64::dgemm_kernel<false, false>);
     if (rc != MGX_SUCCESS) return rc;
     MGX_HOST_CHECK(cudaGetLastError());
+    if (slices > 1) {
+        int rgrid = mgx_sm_count() * 8;
+        if (rgrid > m) rgrid = m;
+        fp64::splitk_reduce<<<rgrid, 256, 0, stream>>>(C, ldc, beta_one, p.partial, p.partial_ld, p.partial_stride,
+                                                       slices, m, n);
+        MGX_HOST_CHECK(cudaGetLastError());
+    }
     return MGX_SUCCESS;
 }
 

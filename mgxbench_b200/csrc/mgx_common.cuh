@@ -25,6 +25,8 @@ void mgx_set_last_cuda_error(cudaError_t e, const char *what, const char *file, 
 void mgx_set_last_message(const char *fmt, ...);
 int *mgx_device_status_ptr();  // device address of this device's status word (no allocation)
 int mgx_sm_count();
+// Stream-ordered scratch from the library's pool on the current device (free with cudaFreeAsync).
+int mgx_scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream);
 int mgx_encode_tmap_2d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_bytes, const void *base,
                        uint64_t inner, uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
                        uint32_t box_outer, CUtensorMapSwizzle swizzle);

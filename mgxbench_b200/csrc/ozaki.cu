@@ -30,6 +30,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <vector>
+
 #include "mgx_common.cuh"
 
 namespace mgx {
@@ -175,9 +177,9 @@ __device__ __forceinline__ size_t slab_offset(int tile, int kb, int kblocks, int
 
 // One warp per (8-row group, K block): lane -> row (lane / 4), 8 consecutive k (lane % 4).
 // Rows up to the 128-row padding and k up to the 32 padding get zero digits.
+template <int S>
 __global__ void __launch_bounds__(256) ozaki_split_a(const double *__restrict__ A, int m, int k, int lda, int mp,
-                                                     int kblocks, int s, const int *__restrict__ ea,
-                                                     uint8_t *__restrict__ da)
+                                                     int kblocks, const int *__restrict__ ea, uint8_t *__restrict__ da)
 {
     const int lane = threadIdx.x & 31;
     const long long wpb = blockDim.x >> 5;
@@ -188,31 +190,32 @@ __global__ void __launch_bounds__(256) ozaki_split_a(const double *__restrict__ 
         const int k0 = kb * 32 + kq * 8;
         int e = (row < m) ? ea[row] : 0;
         if (e == NONFINITE_EXP) e = 0;
-        unsigned long long packed[MAX_SPLITS];
+        unsigned long long packed[S];
 #pragma unroll
-        for (int t = 0; t < MAX_SPLITS; ++t) packed[t] = 0;
+        for (int t = 0; t < S; ++t) packed[t] = 0;
         const double *arow = A + (size_t)(row < m ? row : 0) * lda;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int kk = k0 + j;
             double v = (row < m && kk < k) ? __ldg(arow + kk) : 0.0;
             if (!isfinite(v)) v = 0.0;
-            int8_t dg[MAX_SPLITS];
-            digits<MAX_SPLITS>(v, e, dg, s);
+            int8_t dg[S];
+            digits<S>(v, e, dg, S);
 #pragma unroll
-            for (int t = 0; t < MAX_SPLITS; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
+            for (int t = 0; t < S; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
         }
-        const size_t off = slab_offset(row >> 7, kb, kblocks, s, row & 127, kq * 8);
+        const size_t off = slab_offset(row >> 7, kb, kblocks, S, row & 127, kq * 8);
 #pragma unroll
-        for (int t = 0; t < MAX_SPLITS; ++t)
-            if (t < s) *reinterpret_cast<unsigned long long *>(da + off + (size_t)t * SLICE_TILE_BYTES) = packed[t];
+        for (int t = 0; t < S; ++t)
+            *reinterpret_cast<unsigned long long *>(da + off + (size_t)t * SLICE_TILE_BYTES) = packed[t];
     }
 }
 
 // Block: 32 k x 128 columns of B through shared memory (coalesced reads along the columns),
 // written as the digit tiles of B^T (column j of B is row j of the tile).
+template <int S>
 __global__ void __launch_bounds__(256) ozaki_split_b(const double *__restrict__ B, int k, int n, int ldb, int kblocks,
-                                                     int s, const int *__restrict__ eb, uint8_t *__restrict__ db)
+                                                     const int *__restrict__ eb, uint8_t *__restrict__ db)
 {
     __shared__ double tb[32][129];
     const int tn = blockIdx.x, kb = blockIdx.y;
@@ -230,20 +233,20 @@ __global__ void __launch_bounds__(256) ozaki_split_b(const double *__restrict__ 
         const int r = item >> 2, kq = item & 3;   // tile row r = column n0 + r of B
         int e = (n0 + r < n) ? eb[n0 + r] : 0;
         if (e == NONFINITE_EXP) e = 0;
-        unsigned long long packed[MAX_SPLITS];
+        unsigned long long packed[S];
 #pragma unroll
-        for (int t = 0; t < MAX_SPLITS; ++t) packed[t] = 0;
+        for (int t = 0; t < S; ++t) packed[t] = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            int8_t dg[MAX_SPLITS];
-            digits<MAX_SPLITS>(tb[kq * 8 + j][r], e, dg, s);
+            int8_t dg[S];
+            digits<S>(tb[kq * 8 + j][r], e, dg, S);
 #pragma unroll
-            for (int t = 0; t < MAX_SPLITS; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
+            for (int t = 0; t < S; ++t) packed[t] |= (unsigned long long)(uint8_t)dg[t] << (8 * j);
         }
-        const size_t off = slab_offset(tn, kb, kblocks, s, r, kq * 8);
+        const size_t off = slab_offset(tn, kb, kblocks, S, r, kq * 8);
 #pragma unroll
-        for (int t = 0; t < MAX_SPLITS; ++t)
-            if (t < s) *reinterpret_cast<unsigned long long *>(db + off + (size_t)t * SLICE_TILE_BYTES) = packed[t];
+        for (int t = 0; t < S; ++t)
+            *reinterpret_cast<unsigned long long *>(db + off + (size_t)t * SLICE_TILE_BYTES) = packed[t];
     }
 }
 
@@ -623,6 +626,50 @@ WsLayout ws_layout(int m, int n, int k, int s)
 }  // namespace
 
 // Phase 1: exponents and digit tiles of A (m x k) and B (k x n) into the workspace (k <= kmax).
+// Calls F<S>() for the runtime split count s (2..12).
+template <template <int> class F, typename... Args>
+static int dispatch_splits(int s, Args... args)
+{
+    switch (s) {
+    case 2: return F<2>::run(args...);
+    case 3: return F<3>::run(args...);
+    case 4: return F<4>::run(args...);
+    case 5: return F<5>::run(args...);
+    case 6: return F<6>::run(args...);
+    case 7: return F<7>::run(args...);
+    case 8: return F<8>::run(args...);
+    case 9: return F<9>::run(args...);
+    case 10: return F<10>::run(args...);
+    case 11: return F<11>::run(args...);
+    case 12: return F<12>::run(args...);
+    default:
+        mgx_set_last_message("mgx_gemm_ozaki: %d splits is outside 2..12", s);
+        return MGX_E_INVALID;
+    }
+}
+
+template <int S>
+struct SplitA {
+    static int run(const double *A, int m, int k, int lda, int mp, int kblocks, const int *ea, uint8_t *da,
+                   cudaStream_t stream)
+    {
+        oz::ozaki_split_a<S><<<mgx_sm_count() * 16, 256, 0, stream>>>(A, m, k, lda, mp, kblocks, ea, da);
+        MGX_HOST_CHECK(cudaGetLastError());
+        return MGX_SUCCESS;
+    }
+};
+
+template <int S>
+struct SplitB {
+    static int run(const double *B, int k, int n, int ldb, int np, int kblocks, const int *eb, uint8_t *db,
+                   cudaStream_t stream)
+    {
+        oz::ozaki_split_b<S><<<dim3(np / 128, kblocks), 256, 0, stream>>>(B, k, n, ldb, kblocks, eb, db);
+        MGX_HOST_CHECK(cudaGetLastError());
+        return MGX_SUCCESS;
+    }
+};
+
 static int ozaki_split_a_impl(const double *A, int m, int k, int lda, int s, unsigned char *ws, const WsLayout &L,
                               cudaStream_t stream)
 {
@@ -632,9 +679,7 @@ static int ozaki_split_a_impl(const double *A, int m, int k, int lda, int s, uns
     const int mp = (m + 127) / 128 * 128;
     oz::ozaki_row_exp<<<(m + 7) / 8, 256, 0, stream>>>(A, m, k, lda, ea, status);
     MGX_HOST_CHECK(cudaGetLastError());
-    oz::ozaki_split_a<<<mgx_sm_count() * 16, 256, 0, stream>>>(A, m, k, lda, mp, kblocks, s, ea, ws + L.da);
-    MGX_HOST_CHECK(cudaGetLastError());
-    return MGX_SUCCESS;
+    return dispatch_splits<SplitA>(s, A, m, k, lda, mp, kblocks, (const int *)ea, ws + L.da, stream);
 }
 
 static int ozaki_split_b_impl(const double *B, int n, int k, int ldb, int s, unsigned char *ws, const WsLayout &L,
@@ -654,9 +699,7 @@ static int ozaki_split_b_impl(const double *B, int n, int k, int ldb, int s, uns
     MGX_HOST_CHECK(cudaGetLastError());
     oz::ozaki_col_exp<<<(n + 255) / 256, 256, 0, stream>>>(colmax, n, eb, status);
     MGX_HOST_CHECK(cudaGetLastError());
-    oz::ozaki_split_b<<<dim3(np / 128, kblocks), 256, 0, stream>>>(B, k, n, ldb, kblocks, s, eb, ws + L.db);
-    MGX_HOST_CHECK(cudaGetLastError());
-    return MGX_SUCCESS;
+    return dispatch_splits<SplitB>(s, B, k, n, ldb, np, kblocks, (const int *)eb, ws + L.db, stream);
 }
 
 static int ozaki_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int s,
@@ -857,13 +900,39 @@ extern "C" MGX_API int mgx_ozaki_kmax(int splits)
 }
 
 // ------------------------------------------------------------------------------------------
-// Host-buffer entry point: PCIe copies overlapped with the product, row panel by row panel.
-// B goes to the device first and is sliced once; then for every panel of A rows the copy of
-// the next panel, the slicing and products of this one and the copy-back of the previous C
-// panel run on three streams.  The result is bit-identical to one mgx_gemm_ozaki call (the
-// exponents are per row of A and per column of B).
+// Host-buffer entry point: PCIe copies overlapped with the product in a 2D block schedule.
+//
+// A is cut into row panels A_0..A_{Pm-1} and B into column panels B_0..B_{Pn-1} (multiples of
+// 128 so every panel starts on a tile).  The copy stream sends A_0, B_0, A_1, B_1, ...; at step
+// t the compute streams prepare the new panels (Ozaki: exponents and digit tiles) and compute
+// every block (i, j) with max(i, j) = t, so the product grows as a square and work starts after
+// the first two panels instead of after all of B.  Blocks alternate between two compute streams
+// so one block's last wave overlaps the next block's first, and each finished block is copied
+// back while the rest compute.  Every element is computed by the same kernel arithmetic as in
+// one mgx_gemm_ozaki / mgx_gemm_fp64 call (exponents per row of A and per column of B over the
+// whole K), so the result is bit-identical to it.
 int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                      int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic);
+
+namespace {
+
+// Layout of rows [r0, ...) and columns [c0, ...) of a whole-problem workspace (r0, c0 multiples
+// of 128): the digit tiles, exponents and column maxima of that sub-block.
+WsLayout ws_sub(const WsLayout &L, int r0, int c0, int s)
+{
+    WsLayout S = L;
+    const size_t tile_slab = (size_t)L.kblocks * s * oz::SLICE_TILE_BYTES;
+    S.da = L.da + (size_t)(r0 / 128) * tile_slab;
+    S.db = L.db + (size_t)(c0 / 128) * tile_slab;
+    S.ea = L.ea + sizeof(int) * (size_t)r0;
+    S.eb = L.eb + sizeof(int) * (size_t)c0;
+    S.colmax = L.colmax + sizeof(unsigned long long) * (size_t)c0;
+    return S;
+}
+
+int round_up(int x, int q) { return (x + q - 1) / q * q; }
+
+}  // namespace
 
 extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double *hC, int m, int n, int k, int lda,
                                      int ldb, int ldc, int form, int splits, int panels, void *stream)
@@ -877,28 +946,37 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
     if (m == 0 || n == 0) return MGX_SUCCESS;
     cudaStream_t s0 = (cudaStream_t)stream;
     if (panels < 1) panels = 1;
-    if (panels > m) panels = m;
     const bool ozaki = form == MGX_FORM_OZAKI && k > 0;
     if (ozaki && k > ozaki_kmax(splits)) {
         mgx_set_last_message("mgx_gemm_host: k = %d is above one int32 accumulation (%d) for %d splits", k,
                              ozaki_kmax(splits), splits);
         return MGX_E_UNSUPPORTED;
     }
-    const int prow = (m + panels - 1) / panels;
+    const int prow = round_up((m + panels - 1) / panels, 128), pcol = round_up((n + panels - 1) / panels, 128);
+    const int Pm = (m + prow - 1) / prow, Pn = (n + pcol - 1) / pcol, T = Pm > Pn ? Pm : Pn;
+    auto r_at = [&](int i) { return i * prow < m ? i * prow : m; };
+    auto c_at = [&](int j) { return j * pcol < n ? j * pcol : n; };
     const size_t kk = (size_t)(k > 0 ? k : 1);
-    const WsLayout L = ozaki ? ws_layout(prow, n, k, splits) : WsLayout{};
-    // device buffers: B, two A panels, two C panels, the Ozaki workspace
-    const size_t bB = align256(kk * n * sizeof(double)), bA = align256((size_t)prow * kk * sizeof(double)),
-                 bC = align256((size_t)prow * n * sizeof(double)), bW = ozaki ? L.total : 0;
+    const WsLayout L = ozaki ? ws_layout(m, n, k, splits) : WsLayout{};
+    // device copies of A, B and C, then the Ozaki workspace of the whole product
+    const size_t bA = align256((size_t)m * kk * sizeof(double)), bB = align256(kk * n * sizeof(double)),
+                 bC = align256((size_t)m * n * sizeof(double)), bW = ozaki ? L.total : 0;
     char *mem = nullptr;
-    MGX_HOST_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&mem), bB + 2 * bA + 2 * bC + bW, s0));
-    double *dB = reinterpret_cast<double *>(mem);
-    double *dA[2] = {reinterpret_cast<double *>(mem + bB), reinterpret_cast<double *>(mem + bB + bA)};
-    double *dC[2] = {reinterpret_cast<double *>(mem + bB + 2 * bA), reinterpret_cast<double *>(mem + bB + 2 * bA + bC)};
-    unsigned char *ws = reinterpret_cast<unsigned char *>(mem + bB + 2 * bA + 2 * bC);
+    {
+        const int arc = mgx_scratch_alloc(reinterpret_cast<void **>(&mem), bA + bB + bC + bW, s0);
+        if (arc != MGX_SUCCESS) return arc;
+    }
+    double *dA = reinterpret_cast<double *>(mem);
+    double *dB = reinterpret_cast<double *>(mem + bA);
+    double *dC = reinterpret_cast<double *>(mem + bA + bB);
+    unsigned char *ws = reinterpret_cast<unsigned char *>(mem + bA + bB + bC);
 
-    cudaStream_t sin = nullptr, sout = nullptr;
-    cudaEvent_t ev[8];
+    cudaStream_t sin = nullptr, sout = nullptr, s1 = nullptr;
+    // events: [0] start, [1] s1 done, [2] copies in done, [3] copies out done, then one per A panel,
+    // per B panel, per step (panels prepared) and per block
+    const int nev = 4 + Pm + Pn + T + Pm * Pn;
+    std::vector<cudaEvent_t> ev(nev, nullptr);
+    cudaEvent_t *evA = ev.data() + 4, *evB = evA + Pm, *evS = evB + Pn, *evBlk = evS + T;
     int rc = MGX_SUCCESS;
     auto fail = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && rc == MGX_SUCCESS) {
@@ -908,53 +986,97 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
     };
     fail(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking), "stream");
     fail(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking), "stream");
-    for (int i = 0; i < 8; ++i) fail(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming), "event");
-    // ev[0]: buffers allocated; ev[1,2]: A panel copied; ev[3,4]: C panel computed; ev[5,6]: C panel copied out
+    fail(cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < nev && rc == MGX_SUCCESS; ++i) fail(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming), "event");
     if (rc == MGX_SUCCESS) {
         fail(cudaEventRecord(ev[0], s0), "record");
         fail(cudaStreamWaitEvent(sin, ev[0], 0), "wait");
         fail(cudaStreamWaitEvent(sout, ev[0], 0), "wait");
-        if (k > 0) fail(cudaMemcpy2DAsync(dB, n * sizeof(double), hB, (size_t)ldb * sizeof(double), n * sizeof(double), k,
-                                          cudaMemcpyHostToDevice, s0), "copy B");
-        if (ozaki && rc == MGX_SUCCESS) rc = ozaki_split_b_impl(dB, n, k, n, splits, ws, L, s0);
+        fail(cudaStreamWaitEvent(s1, ev[0], 0), "wait");
     }
-    for (int p = 0; p < panels && rc == MGX_SUCCESS; ++p) {
-        const int r0 = p * prow, rows = (m - r0 < prow) ? m - r0 : prow;
-        if (rows <= 0) break;
-        const int b = p & 1;
-        if (p >= 2) fail(cudaStreamWaitEvent(sin, ev[3 + b], 0), "wait");      // dA[b] free once panel p-2 computed
-        if (k > 0)
-            fail(cudaMemcpy2DAsync(dA[b], kk * sizeof(double), hA + (size_t)r0 * lda, (size_t)lda * sizeof(double),
-                                   kk * sizeof(double), rows, cudaMemcpyHostToDevice, sin), "copy A panel");
-        fail(cudaEventRecord(ev[1 + b], sin), "record");
-        fail(cudaStreamWaitEvent(s0, ev[1 + b], 0), "wait");
-        if (p >= 2) fail(cudaStreamWaitEvent(s0, ev[5 + b], 0), "wait");      // dC[b] free once copied out
-        if (rc != MGX_SUCCESS) break;
-        if (ozaki) {
-            rc = ozaki_split_a_impl(dA[b], rows, k, (int)kk, splits, ws, L, s0);
-            if (rc == MGX_SUCCESS) rc = ozaki_multiply_impl(dC[b], rows, n, k, n, 0, splits, ws, L, s0);
-        } else {
-            rc = mgx_launch_dgemm(dA[b], dB, dC[b], rows, n, k, 0, k, k, (int)kk, n, n, 0, s0, 0);
+    // copies in: A_0, B_0, A_1, B_1, ...
+    for (int t = 0; t < T && rc == MGX_SUCCESS; ++t) {
+        if (t < Pm) {
+            const int r0 = r_at(t), r1 = r_at(t + 1);
+            if (k > 0)
+                fail(cudaMemcpy2DAsync(dA + (size_t)r0 * kk, kk * sizeof(double), hA + (size_t)r0 * lda,
+                                       (size_t)lda * sizeof(double), kk * sizeof(double), r1 - r0,
+                                       cudaMemcpyHostToDevice, sin), "copy A panel");
+            fail(cudaEventRecord(evA[t], sin), "record");
         }
-        fail(cudaEventRecord(ev[3 + b], s0), "record");
-        fail(cudaStreamWaitEvent(sout, ev[3 + b], 0), "wait");
-        fail(cudaMemcpy2DAsync(hC + (size_t)r0 * ldc, (size_t)ldc * sizeof(double), dC[b], n * sizeof(double),
-                               n * sizeof(double), rows, cudaMemcpyDeviceToHost, sout), "copy C panel");
-        fail(cudaEventRecord(ev[5 + b], sout), "record");
+        if (t < Pn) {
+            const int c0 = c_at(t), c1 = c_at(t + 1);
+            if (k > 0)
+                fail(cudaMemcpy2DAsync(dB + c0, (size_t)n * sizeof(double), hB + c0, (size_t)ldb * sizeof(double),
+                                       (size_t)(c1 - c0) * sizeof(double), k, cudaMemcpyHostToDevice, sin),
+                     "copy B panel");
+            fail(cudaEventRecord(evB[t], sin), "record");
+        }
+    }
+    int blk = 0;
+    auto run_block = [&](int bi, int bj) {
+        if (rc != MGX_SUCCESS) return;
+        const int r0 = r_at(bi), r1 = r_at(bi + 1), c0 = c_at(bj), c1 = c_at(bj + 1);
+        cudaStream_t cs = (blk & 1) ? s1 : s0;
+        double *Cb = dC + (size_t)r0 * n + c0;
+        if (ozaki) {
+            const WsLayout S = ws_sub(L, r0, c0, splits);
+            rc = ozaki_multiply_impl(Cb, r1 - r0, c1 - c0, k, n, 0, splits, ws, S, cs);
+        } else {
+            rc = mgx_launch_dgemm(dA + (size_t)r0 * kk, dB + c0, Cb, r1 - r0, c1 - c0, k, 0, k, k, (int)kk, n, n, 0, cs,
+                                  0);
+        }
+        fail(cudaEventRecord(evBlk[blk], cs), "record");
+        fail(cudaStreamWaitEvent(sout, evBlk[blk], 0), "wait");
+        fail(cudaMemcpy2DAsync(hC + (size_t)r0 * ldc + c0, (size_t)ldc * sizeof(double), Cb, (size_t)n * sizeof(double),
+                               (size_t)(c1 - c0) * sizeof(double), r1 - r0, cudaMemcpyDeviceToHost, sout),
+             "copy C block");
+        ++blk;
+    };
+    for (int t = 0; t < T && rc == MGX_SUCCESS; ++t) {
+        // prepare the panels that arrived at this step (on s0, in order)
+        if (t < Pm) {
+            fail(cudaStreamWaitEvent(s0, evA[t], 0), "wait");
+            if (ozaki && rc == MGX_SUCCESS) {
+                const int r0 = r_at(t), r1 = r_at(t + 1);
+                rc = ozaki_split_a_impl(dA + (size_t)r0 * kk, r1 - r0, k, (int)kk, splits, ws, ws_sub(L, r0, 0, splits),
+                                        s0);
+            }
+        }
+        if (t < Pn) {
+            fail(cudaStreamWaitEvent(s0, evB[t], 0), "wait");
+            if (ozaki && rc == MGX_SUCCESS) {
+                const int c0 = c_at(t), c1 = c_at(t + 1);
+                rc = ozaki_split_b_impl(dB + c0, c1 - c0, k, n, splits, ws, ws_sub(L, 0, c0, splits), s0);
+            }
+        }
+        fail(cudaEventRecord(evS[t], s0), "record");
+        fail(cudaStreamWaitEvent(s1, evS[t], 0), "wait");
+        // every block (i, j) with max(i, j) = t
+        if (t < Pm)
+            for (int j = 0; j <= t && j < Pn; ++j) run_block(t, j);
+        if (t < Pn)
+            for (int i = 0; i < t && i < Pm; ++i) run_block(i, t);
     }
     // join the side streams back into the caller's stream, then release the buffers
-    if (sout) {
-        cudaEventRecord(ev[7], sout);
-        cudaStreamWaitEvent(s0, ev[7], 0);
+    if (s1) {
+        cudaEventRecord(ev[1], s1);
+        cudaStreamWaitEvent(s0, ev[1], 0);
     }
     if (sin) {
-        cudaEventRecord(ev[0], sin);
-        cudaStreamWaitEvent(s0, ev[0], 0);
+        cudaEventRecord(ev[2], sin);
+        cudaStreamWaitEvent(s0, ev[2], 0);
+    }
+    if (sout) {
+        cudaEventRecord(ev[3], sout);
+        cudaStreamWaitEvent(s0, ev[3], 0);
     }
     cudaFreeAsync(mem, s0);
-    for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < nev; ++i)
+        if (ev[i]) cudaEventDestroy(ev[i]);
     if (sin) cudaStreamDestroy(sin);
     if (sout) cudaStreamDestroy(sout);
+    if (s1) cudaStreamDestroy(s1);
     return rc;
 }
 

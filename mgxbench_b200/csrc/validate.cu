@@ -199,7 +199,10 @@ int mgx_validate_impl(const double *d_c, size_t count, double expected, double a
     val::ConstAcc h{0, 0, 0};
     if (count > 0) {
         val::ConstAcc *d_acc = nullptr;
-        MGX_HOST_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&d_acc), sizeof(val::ConstAcc), stream));
+        {
+            const int arc = mgx_scratch_alloc(reinterpret_cast<void **>(&d_acc), sizeof(val::ConstAcc), stream);
+            if (arc != MGX_SUCCESS) return arc;
+        }
         cudaError_t e = cudaMemsetAsync(d_acc, 0, sizeof(val::ConstAcc), stream);
         if (e == cudaSuccess) {
             size_t blocks = (count + val::THREADS - 1) / val::THREADS;
@@ -242,7 +245,10 @@ extern "C" MGX_API int mgx_error_vs_dd(const double *A, const double *B, const d
     };
     Scratch *d = nullptr;
     cudaStream_t s = nullptr;
-    MGX_HOST_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&d), sizeof(Scratch), s));
+    {
+        const int arc = mgx_scratch_alloc(reinterpret_cast<void **>(&d), sizeof(Scratch), s);
+        if (arc != MGX_SUCCESS) return arc;
+    }
     Scratch h;
     cudaError_t e = cudaMemsetAsync(d, 0, sizeof(Scratch), s);
     if (e == cudaSuccess) {

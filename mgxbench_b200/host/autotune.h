@@ -1,0 +1,240 @@
+// autotune.h -- the learned cost model's choice of form and split count inside the drop-in
+// executables (MGXBENCH_FORM=auto).
+//
+// The model file is the JSON written by mgxbench_b200.autotune.MlpModel.save: standardisation
+// constants (xmean, xstd, ymean, ystd), the flat parameter vector of the 6 -> 64 -> 64 -> 2 MLP
+// and the candidate list [[tile, splits], ...].  Inference runs on the GPU through
+// mgx_mlp_forward; the rule is the one of mgxbench_b200.autotune.choose: the fastest candidate
+// whose predicted normwise error meets the target, else the candidate with the most splits.
+// MGXBench's own AUTO mode (autotuning/predictive.py:606-657) chooses a communication library
+// from a regression of measured times; here the choice is the kernel configuration.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <unistd.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "mgxgemm.h"
+
+namespace mm {
+
+struct AutoChoice {
+    int form = -1;        // MGX_FORM_FP64 or MGX_FORM_OZAKI
+    int splits = 0;
+    int ksplit = 1;       // FP64 split-K slices
+    double predicted_s = 0.0;
+    double predicted_err = 0.0;
+    std::string model_path;
+};
+
+// Numbers of the JSON array stored under "key" (the model file is written by this project, so
+// a flat scan for the key and its bracketed list is enough; nested lists are flattened).
+inline bool json_numbers(const std::string &text, const char *key, std::vector<double> *out)
+{
+    const std::string k = std::string("\"") + key + "\"";
+    size_t p = text.find(k);
+    if (p == std::string::npos) return false;
+    p = text.find(':', p + k.size());
+    if (p == std::string::npos) return false;
+    p = text.find_first_not_of(" \t\r\n", p + 1);
+    if (p == std::string::npos || text[p] != '[') return false;
+    int depth = 0;
+    out->clear();
+    const char *s = text.c_str();
+    for (size_t i = p; i < text.size(); ++i) {
+        const char c = s[i];
+        if (c == '[') {
+            ++depth;
+        } else if (c == ']') {
+            if (--depth == 0) return true;
+        } else if (c == '-' || c == '+' || c == '.' || (c >= '0' && c <= '9')) {
+            char *end = nullptr;
+            const double v = strtod(s + i, &end);
+            if (end == s + i) return false;
+            out->push_back(v);
+            i = (size_t)(end - s) - 1;
+        }
+    }
+    return false;
+}
+
+// Directory of this executable (for the default model path).
+inline std::string exe_dir()
+{
+    char buf[4096];
+    const ssize_t n = readlink("/proc/self/exe", buf, sizeof buf - 1);
+    if (n <= 0) return ".";
+    buf[n] = '\0';
+    std::string p(buf);
+    const size_t slash = p.rfind('/');
+    return slash == std::string::npos ? std::string(".") : p.substr(0, slash);
+}
+
+inline std::string default_model_path() { return exe_dir() + "/../mgxbench_b200/data/mlp_b200.json"; }
+
+// Tile ids of the candidates (mgxbench_b200.autotune): 1 is the Ozaki kernel; 0, 2, 3, 4, 5 are
+// the FP64 kernel with the K range cut into 1, 2, 4, 8, 16 slices.
+inline int tile_ksplit(int tile)
+{
+    switch (tile) {
+    case 2: return 2;
+    case 3: return 4;
+    case 4: return 8;
+    case 5: return 16;
+    default: return 1;
+    }
+}
+
+inline bool tile_is_fp64(int tile) { return tile != 1; }
+
+// Same rule as mgxbench_b200.autotune.splitk_applies: each slice gets a 32-wide K block and the
+// partial products fit 4 GiB.
+inline bool splitk_applies(int m, int n, int k, int ksplit)
+{
+    return ksplit == 1 || ((k + 31) / 32 >= ksplit && (double)ksplit * m * n * 8.0 <= 4294967296.0);
+}
+
+// Loads the model at `path` and picks the form and split count for an m x n x k product whose
+// inputs span `exp_range` binades either side of 1.  Returns 0, or a message in *why.
+inline int auto_choose(const std::string &path, int m, int n, int k, double exp_range, double target,
+                       AutoChoice *out, std::string *why, bool whole_k_only = false)
+{
+    std::ifstream f(path);
+    if (!f) {
+        *why = "cannot read cost model " + path;
+        return -1;
+    }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    if (text.find("\"mgx-mlp-v1\"") == std::string::npos) {
+        *why = path + " is not an mgx-mlp-v1 model";
+        return -1;
+    }
+    std::vector<double> xmean, xstd, ymean, ystd, params, cand;
+    if (!json_numbers(text, "xmean", &xmean) || !json_numbers(text, "xstd", &xstd) ||
+        !json_numbers(text, "ymean", &ymean) || !json_numbers(text, "ystd", &ystd) ||
+        !json_numbers(text, "params", &params) || xmean.size() != 6 || xstd.size() != 6 || ymean.size() != 2 ||
+        ystd.size() != 2 || (int)params.size() != mgx_mlp_param_count()) {
+        *why = path + ": missing or mis-sized model arrays";
+        return -1;
+    }
+    if (!json_numbers(text, "candidates", &cand) || cand.empty() || cand.size() % 2) {
+        cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0};  // default list: FP64 (1..16 K slices), Ozaki 3..9 splits
+        for (int s = 3; s <= 9; ++s) {
+            cand.push_back(1);
+            cand.push_back(s);
+        }
+    }
+    {   // keep the candidates that apply to this product
+        std::vector<double> keep;
+        for (size_t c = 0; c + 1 < cand.size(); c += 2) {
+            const int ks = tile_is_fp64((int)cand[c]) ? tile_ksplit((int)cand[c]) : 1;
+            if (!splitk_applies(m, n, k, ks) || (whole_k_only && ks > 1)) continue;
+            keep.push_back(cand[c]);
+            keep.push_back(cand[c + 1]);
+        }
+        cand.swap(keep);
+    }
+    const int nc = (int)cand.size() / 2;
+    if (nc == 0) {
+        *why = path + ": no candidate applies to this product";
+        return -1;
+    }
+    std::vector<float> X((size_t)nc * 6), P(params.begin(), params.end()), Y((size_t)nc * 2);
+    for (int c = 0; c < nc; ++c) {
+        const double feat[6] = {std::log2((double)m), std::log2((double)n), std::log2((double)k), exp_range,
+                                cand[2 * c], cand[2 * c + 1]};
+        for (int j = 0; j < 6; ++j) X[(size_t)c * 6 + j] = (float)((feat[j] - xmean[j]) / xstd[j]);
+    }
+    float *dX = nullptr, *dP = nullptr, *dY = nullptr;
+    int rc = 0;
+    if (cudaMalloc(&dX, X.size() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&dP, P.size() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&dY, Y.size() * sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(dX, X.data(), X.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dP, P.data(), P.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        *why = "cannot stage the cost model on the device";
+        rc = -1;
+    }
+    if (rc == 0 && mgx_mlp_forward(dX, nc, dP, dY, nullptr) != MGX_SUCCESS) {
+        *why = std::string("cost model inference failed: ") + mgx_last_error_message();
+        rc = -1;
+    }
+    if (rc == 0 && cudaMemcpy(Y.data(), dY, Y.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        *why = "cannot read the cost model's predictions";
+        rc = -1;
+    }
+    cudaFree(dX);
+    cudaFree(dP);
+    cudaFree(dY);
+    if (rc) return rc;
+    int best = -1, most = -1;
+    double best_t = 0.0;
+    for (int c = 0; c < nc; ++c) {
+        const double t = std::exp(Y[(size_t)c * 2] * ystd[0] + ymean[0]);
+        const double e = std::pow(10.0, Y[(size_t)c * 2 + 1] * ystd[1] + ymean[1]);
+        if (e <= target && (best < 0 || t < best_t)) {
+            best = c;
+            best_t = t;
+        }
+        // fallback: most splits, then the lowest tile id (mgxbench_b200.autotune.choose)
+        if (most < 0 || cand[2 * c + 1] > cand[2 * most + 1] ||
+            (cand[2 * c + 1] == cand[2 * most + 1] && cand[2 * c] < cand[2 * most]))
+            most = c;
+    }
+    const int pick = best >= 0 ? best : most;
+    out->form = tile_is_fp64((int)cand[2 * pick]) ? MGX_FORM_FP64 : MGX_FORM_OZAKI;
+    out->splits = (int)cand[2 * pick + 1];
+    out->ksplit = tile_is_fp64((int)cand[2 * pick]) ? tile_ksplit((int)cand[2 * pick]) : 1;
+    out->predicted_s = std::exp(Y[(size_t)pick * 2] * ystd[0] + ymean[0]);
+    out->predicted_err = std::pow(10.0, Y[(size_t)pick * 2 + 1] * ystd[1] + ymean[1]);
+    out->model_path = path;
+    return 0;
+}
+
+// Normwise error target of the automatic choice (MGXBENCH_TARGET_ERR, default 1e-15); the
+// executables also validate an automatically chosen form against it.
+inline double auto_target()
+{
+    const char *t = getenv("MGXBENCH_TARGET_ERR");
+    return (t && *t) ? atof(t) : 1e-15;
+}
+
+// MGXBENCH_FORM=auto: replaces *form / *splits / *form_name with the cost model's choice for an
+// m x n x k product and prints it.  The model is MGXBENCH_AUTO_MODEL (default
+// ../mgxbench_b200/data/mlp_b200.json beside the executable); the target is
+// MGXBENCH_TARGET_ERR (normwise, default 1e-15).  Exits with `exit_code` if the model is
+// unusable: AUTO without a model is an error, as in MGXBench (autotuning/predictive.py:609-611).
+inline void resolve_auto_form(int *form, int *splits, int *ksplit, std::string *form_name, int m, int n, int k,
+                              double exp_range, int exit_code, bool whole_k_only)
+{
+    if (*form != 2) return;
+    const char *env = getenv("MGXBENCH_AUTO_MODEL");
+    const std::string path = (env && *env) ? std::string(env) : default_model_path();
+    const double target = auto_target();
+    AutoChoice c;
+    std::string why;
+    if (auto_choose(path, m, n, k, exp_range, target, &c, &why, whole_k_only) != 0) {
+        fprintf(stderr, "AUTO: %s\n", why.c_str());
+        fflush(stderr);
+        exit(exit_code);
+    }
+    *form = c.form == MGX_FORM_OZAKI ? 1 : 0;
+    *splits = c.form == MGX_FORM_OZAKI ? c.splits : 0;
+    *ksplit = c.ksplit;
+    *form_name = c.form == MGX_FORM_OZAKI ? "ozaki" : "fp64";
+    printf("mmb autotune: model=%s m=%d n=%d k=%d exp_range=%g target=%.3e choice=%s splits=%d ksplit=%d "
+           "predicted_s=%.6e predicted_err=%.3e\n",
+           path.c_str(), m, n, k, exp_range, target, form_name->c_str(), *splits, *ksplit, c.predicted_s,
+           c.predicted_err);
+}
+
+}  // namespace mm

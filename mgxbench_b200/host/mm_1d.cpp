@@ -13,6 +13,7 @@
 // (mmb.cu:937), the NUMERICAL VALIDATION block (mulmat_kernel.cu:298-319) and one
 // BENCHMARK_RESULT line (mmb.cu:964-965); exit status 0 when valid, 2 otherwise (mmb.cu:1036).
 // Keys this build adds come after the reference's keys on the same line.
+#include "autotune.h"
 #include "mm_common.h"
 
 static int pipeline_k_chunk_from_env(int k)  // 1D-row-block/mmb.cu:109-128
@@ -61,9 +62,9 @@ int main(int argc, char *argv[])
     }
     std::string input_name, form_name;
     const int input = mm::input_kind(&input_name);
-    const int form = mm::compute_form(&form_name);
+    int form = mm::compute_form(&form_name);
     if (input < 0 || form < 0) {
-        fprintf(stderr, "MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki\n");
+        fprintf(stderr, "MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|auto\n");
         return EXIT_FAILURE;
     }
     mm::cuda_or_die(cudaSetDevice(deviceId), "cudaSetDevice", EXIT_FAILURE);
@@ -79,7 +80,13 @@ int main(int argc, char *argv[])
     const int pipeline_k_chunk = pipeline_k_chunk_from_env(k);
     const char libB = libs[1];
     const bool chunked = (libB == 'S' || libB == 'Y' || libB == 'X');
-    const int splits = mm::env_int("MGXBENCH_SPLITS", 8);
+    int splits = mm::env_int("MGXBENCH_SPLITS", 8);
+    int ksplit = mm::env_int("MGXBENCH_KSPLIT", 1);
+    const bool autotuned = form == mm::kAuto;
+    // the choice is made for the product each emulated rank runs (its K chunk when chunked)
+    mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, mi, n, chunked ? std::min(pipeline_k_chunk, k) : k,
+                          input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, EXIT_FAILURE, chunked);
+    if (chunked || form != mm::kFp64) ksplit = 1;
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
     printf("mmb one-GPU emulation: ranks=%d rows/rank=%d form=%s%s input=%s B-structure=%s", nRanks, mi,
            form_name.c_str(), form == mm::kOzaki ? (std::string(" splits=") + std::to_string(splits)).c_str() : "",
@@ -125,12 +132,12 @@ int main(int argc, char *argv[])
                         rc = mgx_ab_multiply_accumulate_async(A_r, d_B + (size_t)k_offset * n, C_r, mi, n, k, k_offset,
                                                               kc, k, n, n, 32, stream);
                     else
-                        rc = mm::block_gemm(form, splits, ws, A_r + k_offset, d_B + (size_t)k_offset * n, C_r, mi, n,
+                        rc = mm::block_gemm(form, splits, 1, ws, A_r + k_offset, d_B + (size_t)k_offset * n, C_r, mi, n,
                                             kc, k, n, n, 1, stream);
                     if (rc < 0) return rc;
                 }
             } else {
-                const int rc = mm::block_gemm(form, splits, ws, A_r, d_B, C_r, mi, n, k, k, n, n, 0, stream);
+                const int rc = mm::block_gemm(form, splits, ksplit, ws, A_r, d_B, C_r, mi, n, k, k, n, n, 0, stream);
                 if (rc < 0) return rc;
             }
         }
@@ -190,7 +197,7 @@ int main(int argc, char *argv[])
         const int v = mgx_validate_matrix_c(d_C, m, n, expected_C, 1.0e-9, 1.0e-12, myRank, 1, nullptr);
         all_valid = (v == 1);
     } else {
-        const double tol = form == mm::kOzaki ? 1e-15 : 1e-12;
+        const double tol = autotuned ? mm::auto_target() : form == mm::kOzaki ? 1e-15 : 1e-12;
         all_valid = mm::report_accuracy(d_A, d_B, d_C, m, n, k, mm::env_int("MGXBENCH_CHECK_ROWS", 256), tol, &err);
     }
     if (dev_status != 0) {
@@ -203,6 +210,7 @@ int main(int argc, char *argv[])
            libs, matrix_size, nRanks, avg_time_execution, all_valid, loop_count, form_name.c_str(), tflops,
            input_name.c_str());
     if (form == mm::kOzaki) printf(" splits=%d", splits);
+    if (ksplit > 1) printf(" ksplit=%d", ksplit);
     if (input != mm::kConst) printf(" norm_rel_err=%.3e max_rel_err=%.3e", err.normwise, err.max_rel);
     printf("\n");
     fflush(stdout);

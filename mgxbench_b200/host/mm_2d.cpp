@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <climits>
 
+#include "autotune.h"
 #include "mm_common.h"
 
 static void fail(const char *message)
@@ -104,9 +105,13 @@ int main(int argc, char **argv)
 
     std::string input_name, form_name;
     const int input = mm::input_kind(&input_name);
-    const int form = mm::compute_form(&form_name);
-    if (input < 0 || form < 0) fail("MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki");
-    const int splits = mm::env_int("MGXBENCH_SPLITS", 8);
+    int form = mm::compute_form(&form_name);
+    if (input < 0 || form < 0) fail("MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|auto");
+    int splits = mm::env_int("MGXBENCH_SPLITS", 8);
+    int ksplit = 1;  // the SUMMA panels are the K split
+    const bool autotuned = form == mm::kAuto;
+    mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, M, Ncols, K,
+                          input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, 2, true);
     const int persistent = mm::env_int("MGXBENCH_PERSISTENT", 1);
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
 
@@ -167,7 +172,7 @@ int main(int argc, char **argv)
             for (int bi = 0; bi < Pr; ++bi)
                 for (int bj = 0; bj < Pc; ++bj) {
                     const int r0 = rcut[bi], c0 = ccut[bj];
-                    const int rc = mm::block_gemm(form, splits, ws, dA + (size_t)r0 * K, dB + c0, dC + (size_t)r0 * Ncols + c0,
+                    const int rc = mm::block_gemm(form, splits, 1, ws, dA + (size_t)r0 * K, dB + c0, dC + (size_t)r0 * Ncols + c0,
                                                   rcut[bi + 1] - r0, ccut[bj + 1] - c0, K, K, Ncols, Ncols, 1, stream);
                     if (rc < 0) return rc;
                 }
@@ -241,7 +246,7 @@ int main(int argc, char **argv)
                     }
             }
     } else {
-        const double tol = form == mm::kOzaki ? 1e-15 : 1e-12;
+        const double tol = autotuned ? mm::auto_target() : form == mm::kOzaki ? 1e-15 : 1e-12;
         valid = mm::report_accuracy(dA, dB, dC, M, Ncols, K, mm::env_int("MGXBENCH_CHECK_ROWS", 256), tol, &err);
     }
     if (dev_status != 0) {

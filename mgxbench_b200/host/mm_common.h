@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -59,14 +60,16 @@ inline int input_kind(std::string *name)
     return -1;
 }
 
-// Compute forms (MGXBENCH_FORM): native FP64 tensor-core MMA or the Ozaki INT8 form.
-enum Form { kFp64 = 0, kOzaki = 1 };
+// Compute forms (MGXBENCH_FORM): native FP64 tensor-core MMA, the Ozaki INT8 form, or "auto"
+// (the learned cost model picks one of the two and the split count, see autotune.h).
+enum Form { kFp64 = 0, kOzaki = 1, kAuto = 2 };
 
 inline int compute_form(std::string *name)
 {
     *name = env_str("MGXBENCH_FORM", "fp64");
     if (*name == "fp64") return kFp64;
     if (*name == "ozaki") return kOzaki;
+    if (*name == "auto") return kAuto;
     return -1;
 }
 
@@ -109,10 +112,16 @@ struct Workspace {
     }
 };
 
-// One block multiply C (+)= A B of the selected form.
-inline int block_gemm(int form, int splits, Workspace &ws, const double *A, const double *B, double *C, int m,
-                      int n, int k, int lda, int ldb, int ldc, int beta_one, cudaStream_t s)
+// One block multiply C (+)= A B of the selected form (FP64 with `ksplit` K slices).
+inline int block_gemm(int form, int splits, int ksplit, Workspace &ws, const double *A, const double *B, double *C,
+                      int m, int n, int k, int lda, int ldb, int ldc, int beta_one, cudaStream_t s)
 {
+    if (form == kFp64 && ksplit > 1) {
+        const size_t need = mgx_fp64_splitk_workspace_size(m, n, k, ksplit);
+        void *w = ws.get(need);
+        if (!w && need) return MGX_E_CUDA;
+        return mgx_gemm_fp64_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one, ksplit, w, need, s);
+    }
     if (form == kFp64) return mgx_gemm_fp64(A, B, C, m, n, k, lda, ldb, ldc, beta_one, s);
     const size_t need = mgx_ozaki_workspace_size(m, n, k, splits);
     void *w = ws.get(need);

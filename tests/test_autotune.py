@@ -14,9 +14,12 @@ def synthetic_rows(shapes, seed=0):
     rows = []
     for (m, n, k, er) in shapes:
         f = 2.0 * m * n * k
-        for c in at.candidates():
-            if c.tile == at.TILE_FP64:
-                t, e = f / 30e12, 1e-15 * math.sqrt(k / 1e3)
+        for c in at.candidates(m, n, k):
+            if c.is_fp64:
+                # split-K helps only products with few output tiles
+                tiles = math.ceil(m / 128) * math.ceil(n / 128)
+                t = f / 30e12 * max(1.0, 148 / tiles) / min(c.ksplit, max(1.0, 148 / tiles)) + 3e-6 * c.ksplit
+                e = 1e-15 * math.sqrt(k / 1e3 / c.ksplit)
             else:
                 t = f * c.splits * (c.splits + 1) / 2 / 4.5e15 + 8.0 * (m * k + k * n) / 3e12
                 e = max(10.0 ** (-8 - 2 * (c.splits - 4)) * (1 if er > 8 else 0.1), 5e-17)
@@ -28,10 +31,17 @@ def synthetic_rows(shapes, seed=0):
 
 def test_candidates_and_features():
     cs = at.candidates()
-    assert cs[0].tile == at.TILE_FP64 and cs[0].splits == 0
-    assert [c.splits for c in cs[1:]] == list(range(3, 10))
-    f = at.features(1024, 2048, 4096, 20, cs[3])
+    assert cs[0].tile == at.TILE_FP64 and cs[0].splits == 0 and cs[0].ksplit == 1
+    assert [c.ksplit for c in cs if c.is_fp64] == [1, 2, 4, 8, 16]
+    assert [c.splits for c in cs if not c.is_fp64] == list(range(3, 10))
+    oz5 = next(c for c in cs if c.splits == 5)
+    f = at.features(1024, 2048, 4096, 20, oz5)
     assert f[:3] == [10.0, 11.0, 12.0] and f[3:] == [20.0, 1.0, 5.0]
+    # split-K candidates only where the K range has the blocks and the slices fit the workspace cap
+    small = at.candidates(300, 300, 100)            # 4 K blocks
+    assert [c.ksplit for c in small if c.is_fp64] == [1, 2, 4]
+    big = at.candidates(32768, 32768, 32768)
+    assert [c.ksplit for c in big if c.is_fp64] == [1]
 
 
 def test_random_shapes_and_memory_bound():

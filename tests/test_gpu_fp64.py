@@ -133,3 +133,41 @@ def test_reference_kernels_pin_the_oracle(mgx, oracle):
         Cacc = C0.copy()
         oracle.ab_multiply_accumulate(A, B[kc:], Cacc, kc, k - kc)
         assert np.array_equal(bits(host(dC3)), bits(Cacc))
+
+
+@pytest.mark.parametrize("m,n,k,ks", [(200, 150, 2000, 4), (129, 257, 300, 2), (7, 9, 13, 8), (333, 127, 1000, 16),
+                                      (256, 256, 4096, 64), (64, 64, 64, 3)])
+def test_splitk_matches_oracle(mgx, oracle, m, n, k, ks):
+    """Split-K: each slice is an FP64 sum, slices summed in order; the any-order bound still holds."""
+    import torch
+    rng = np.random.default_rng(m * 3 + n + k + ks)
+    A, B = rng_matrix(rng, (m, k)), rng_matrix(rng, (k, n))
+    dA, dB = dev(A), dev(B)
+    dC = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_fp64(dA, dB, dC, ksplit=ks)
+    check_close(host(dC), A, B, oracle, k)
+    # deterministic: slices are reduced in a fixed order
+    dC2 = torch.empty_like(dC)
+    mgx.gemm_fp64(dA, dB, dC2, ksplit=ks)
+    assert np.array_equal(bits(host(dC)), bits(host(dC2)))
+    assert mgx.device_status() == 0
+
+
+def test_splitk_accumulates_and_checks_workspace(mgx, oracle):
+    import ctypes
+    import torch
+    rng = np.random.default_rng(5)
+    m, n, k = 150, 98, 1500
+    A, B, C0 = rng_matrix(rng, (m, k)), rng_matrix(rng, (k, n)), rng_matrix(rng, (m, n))
+    dC = dev(C0)
+    mgx.gemm_fp64(dev(A), dev(B), dC, beta_one=True, ksplit=6)
+    ref = C0 + oracle.ab_multiply(A, B)
+    _, _, ab = oracle.gemm_dd(A, B)
+    assert np.all(np.abs(host(dC) - ref) <= 2 * gamma(k + 1) * (ab + np.abs(C0)) + 1e-300)
+    need = mgx.fp64_splitk_workspace_size(m, n, k, 6)
+    assert need >= 6 * m * n * 8
+    assert mgx.fp64_splitk_workspace_size(m, n, 31, 6) == 0  # one K block: one slice
+    small = torch.empty(need // 2, dtype=torch.uint8, device="cuda")
+    rc = mgx.lib().mgx_gemm_fp64_splitk(vp(dev(A)), vp(dev(B)), vp(dC), m, n, k, k, n, n, 0, 6, vp(small),
+                                        small.numel(), None)
+    assert rc == -5  # MGX_E_WORKSPACE

@@ -97,13 +97,15 @@ def test_ozaki_k_beyond_int32_headroom(mgx, oracle):
     assert np.array_equal(bits(host(dC)), bits(oracle.ozaki_gemm(A, B, s)))
 
 
-@pytest.mark.parametrize("form,panels", [(1, 1), (1, 3), (0, 4)])
-def test_host_buffer_entry_point_matches_device_path(mgx, oracle, form, panels):
-    """mgx_gemm_host (PCIe copies overlapped with the product, row panel by row panel) gives the
-    same bits as the device-buffer entry points."""
+@pytest.mark.parametrize("form,panels,m,n,k", [(1, 1, 333, 270, 515), (1, 3, 333, 270, 515), (0, 4, 333, 270, 515),
+                                               (1, 4, 700, 201, 300), (0, 4, 700, 201, 300), (1, 10, 129, 1000, 64),
+                                               (0, 2, 1, 1, 1)])
+def test_host_buffer_entry_point_matches_device_path(mgx, oracle, form, panels, m, n, k):
+    """mgx_gemm_host (PCIe copies overlapped with the product in a 2D block schedule: row panels
+    of A x column panels of B, uneven panels, odd n) gives the same bits as the device-buffer
+    entry points, and writes every element of C."""
     import torch
-    rng = np.random.default_rng(11)
-    m, n, k = 333, 270, 515
+    rng = np.random.default_rng(11 + m + n)
     A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
     hA = torch.from_numpy(A).pin_memory()
     hB = torch.from_numpy(B).pin_memory()
