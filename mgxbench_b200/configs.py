@@ -6,8 +6,8 @@ each (python -m mgxbench_b200.configs [cfg1 cfg2 cfg3 cfg4 cfg5]).
   cfg3  Ozaki N = 16384, u * 2^e (e in [-20, 20]), split count swept 3..9, native FP64 beside
   cfg4  2D SUMMA M = 12288, N = 20480, K = 16384, 3 x 5 grid, panel width 512, FP64 and Ozaki
         forms, each one persistent plan replayed from a CUDA graph
-  cfg5  learned cost model: regret against the exhaustive sweep (needs a sweep database and a
-        trained model, see mgxbench_b200.autotune)
+  cfg5  learned cost model: regret against the exhaustive sweep and prediction accuracy, beside
+        the regression baseline (the packaged sweep database and model, or the files given)
 
 Times are CUDA events on the launching stream after warm-up; errors are against the GPU
 double-double product (all rows for cfg1, sampled rows otherwise).  Inputs are seeded synthetic
@@ -102,18 +102,24 @@ class _Fixed:
         return self.t
 
 
-def cfg4(splits=None, model=None):
+def cfg4(splits=None, model="default"):
+    """The Ozaki plan's split count comes from the packaged learned cost model (the autotuner)
+    when it is present, else from the a-priori error model."""
     M, N, K, pr, pc, bk = 12288, 20480, 16384, 3, 5, 512
     A, B = _mat(M, K, 1, 41), _mat(K, N, 1, 42)
     C = torch.empty((M, N), dtype=torch.float64, device="cuda")
+    chooser = "ozaki_choose_splits"
     if splits is None:
         splits = mgx.ozaki_choose_splits(K, 0.0, 1e-15)
+        from mgxbench_b200 import autotune as at
+        from mgxbench_b200 import predictive as pr_mod
+        if model == "default":
+            model = at.MlpModel.load(pr_mod.DEFAULT_MODEL) if pr_mod.DEFAULT_MODEL.is_file() else None
         if model is not None:
-            from mgxbench_b200 import autotune as at
             plan_cands = [c for c in at.candidates() if c.ksplit == 1]  # SUMMA panels are the K split
-            c = at.choose(model, M, N, K, 0, 1e-15, plan_cands)
-            if not c.is_fp64:
-                splits = c.splits
+            oz = [c for c in plan_cands if not c.is_fp64]
+            splits = at.choose(model, M, N, K, 0, 1e-15, oz).splits
+            chooser = "learned cost model"
     out = []
     for form, s in ((mgx.FORM_FP64, 0), (mgx.FORM_OZAKI, splits)):
         plan = mgx.SummaPlan(M, N, K, pr, pc, bk, form=form, splits=max(s, 2))
@@ -130,25 +136,30 @@ def cfg4(splits=None, model=None):
                     "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}", "panel_k": bk, "panels": info["panels"],
                     "work_tiles": info["work_tiles"], "tflops": 2 * M * N * K / t / 1e12, "seconds": t,
                     "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": True,
-                    "persistent_launches_per_product": 1})
+                    "persistent_launches_per_product": 1, "splits_from": chooser if s else None})
         del g
         plan.close()
     return out
 
 
-def cfg5(db_path, model_path, target=1e-15):
+def cfg5(db_path=None, model_path=None):
+    """Regret (at 1e-15 and looser targets) and prediction accuracy of the learned model and of
+    the regression baseline on the exhaustively measured held-out shapes."""
     from mgxbench_b200 import autotune as at
-    db = at.SweepDB(db_path)
+    from mgxbench_b200 import predictive as pr_mod
+    db = at.SweepDB(db_path or pr_mod.DEFAULT_DB)
     train = [r for r in db.rows if r.get("set") == "train"]
     held = [r for r in db.rows if r.get("set") == "heldout"]
-    mlp = at.MlpModel.load(model_path)
-    return {"config": "cfg5", "train_rows": len(train), "heldout_rows": len(held),
-            "mlp": at.regret(mlp, held, target), "regression": at.regret(at.RegressionModel().fit(train), held, target)}
+    mlp = at.MlpModel.load(model_path or pr_mod.DEFAULT_MODEL)
+    return {"config": "cfg5", "train_rows": len(train),
+            "heldout_shapes": len({(r["m"], r["n"], r["k"], r["exp_range"]) for r in held}),
+            "heldout_rows": len(held), "mlp": at.evaluate(mlp, held),
+            "regression": at.evaluate(at.RegressionModel().fit(train), held)}
 
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
-    which = [a for a in argv if a.startswith("cfg")] or ["cfg1", "cfg2", "cfg3", "cfg4"]
+    which = [a for a in argv if a.startswith("cfg")] or ["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"]
     for w in which:
         if w == "cfg5":
             res = cfg5(*[a for a in argv if not a.startswith("cfg")][:2])
