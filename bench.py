@@ -124,6 +124,17 @@ def cpu_reference_rate(n: int, budget_s: float, threads: int = 0):
     return B, rows, rate
 
 
+def ranks_reduce_max(dist, value: float, device) -> float:
+    """Max of a per-rank number over all ranks: a multi-GPU step takes as long as its slowest
+    rank.  `dist` is None for a single process."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
@@ -217,11 +228,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
-    elapsed_ms = t_start.elapsed_time(t_stop)
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = t.item()
+    elapsed_ms = ranks_reduce_max(dist, t_start.elapsed_time(t_stop), "cuda")
     ms_per_step = elapsed_ms / args.steps
     value = world * flop / (ms_per_step * 1e-3) / 1e12
 
@@ -276,11 +283,7 @@ def run_ours(args):
             mgx.gemm_host(hA, hB, hC, form=mgx.FORM_OZAKI, splits=splits, panels=args.panels, stream=stream)
         e1.record(stream)
         e1.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / reps
-        if dist is not None:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = t.item()
+        e2e_ms = ranks_reduce_max(dist, e0.elapsed_time(e1) / reps, "cuda")
         same = bool(torch.equal(hC[probe_rows].view(torch.int64), c_probe.view(torch.int64)))
         e2e = {"value": world * flop / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8, "ms_per_step": e2e_ms,

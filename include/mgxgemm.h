@@ -261,6 +261,11 @@ MGX_API int mgx_mlp_adam_step(float *params, const float *grads, float *m, float
  * Library state
  * ------------------------------------------------------------------------------------------ */
 
+/* Returns the device memory the library keeps cached for its scratch (operand packing, the
+ * host-buffer pipeline) on the current device: it synchronises the device, then releases the
+ * cache.  Later calls allocate again.  No counterpart in MGXBench. */
+MGX_API int mgx_scratch_trim(void);
+
 /* Reads and clears the current device's status word written by bounded device-side waits
  * (0 = none).  Synchronises the device. */
 MGX_API int mgx_device_status(int *code_out);

@@ -79,6 +79,7 @@ EXPORTS = [
     ("mgx_error_vs_dd", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _d, ctypes.POINTER(ErrorReport)]),
     ("mgx_fill_matrix", _i, [_vp, _i, _i, _i, _i, _d, _i, _u64, _vp]),
     ("mgx_device_status", _i, [ctypes.POINTER(_i)]),
+    ("mgx_scratch_trim", _i, []),
     ("mgx_last_error_message", ctypes.c_char_p, []),
     ("mgx_status_string", ctypes.c_char_p, [_i]),
     ("mgx_peak_fp64", _i, [_i, _i, ctypes.POINTER(_d)]),
@@ -234,6 +235,11 @@ def ozaki_multiply(C, k: int, splits: int, workspace, beta_one: bool = False, st
     m, n = C.shape
     return _check(lib().mgx_ozaki_multiply(_ptr(C), m, n, k, _ld(C), int(beta_one), splits, _ptr(workspace),
                                            workspace.numel(), _stream(stream)), "mgx_ozaki_multiply")
+
+
+def scratch_trim():
+    """Release the device memory the library keeps cached for its scratch on this device."""
+    return _check(lib().mgx_scratch_trim(), "mgx_scratch_trim")
 
 
 def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=8, stream=None):

@@ -69,10 +69,10 @@ int mgx_sm_count()
 }
 
 // The library's own stream-ordered memory pool on each device, for short-lived scratch (operand
-// packing, the host-buffer pipeline, validation accumulators).  It keeps up to 8 GiB across
+// packing, the host-buffer pipeline, validation accumulators).  It keeps up to 32 GiB across
 // synchronisations, so repeated calls reuse their scratch instead of mapping fresh memory each
 // time (a process's default pool returns everything at every synchronisation), and it leaves
-// the process's default pool settings alone.
+// the process's default pool settings alone.  mgx_scratch_trim() hands the cached memory back.
 static cudaMemPool_t g_pool[kMaxDevices];
 
 int mgx_scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream)
@@ -94,7 +94,7 @@ int mgx_scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream)
                 mgx_set_last_cuda_error(e, "cudaMemPoolCreate", __FILE__, __LINE__);
                 return MGX_E_CUDA;
             }
-            uint64_t keep = 8ull << 30;
+            uint64_t keep = 32ull << 30;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
             g_pool[dev] = pool;
         }
@@ -104,6 +104,21 @@ int mgx_scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream)
         mgx_set_last_cuda_error(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
         return MGX_E_CUDA;
     }
+    return MGX_SUCCESS;
+}
+
+MGX_API int mgx_scratch_trim(void)
+{
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices) return MGX_E_CUDA;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        pool = g_pool[dev];
+    }
+    if (!pool) return MGX_SUCCESS;
+    MGX_HOST_CHECK(cudaDeviceSynchronize());
+    MGX_HOST_CHECK(cudaMemPoolTrimTo(pool, 0));
     return MGX_SUCCESS;
 }
 

@@ -244,28 +244,57 @@ __global__ void __launch_bounds__(THREADS, 1)
     // slice of the partial products).
     auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int n_lo, int beta_one,
                          double *dst_base, int ld, int vec_store) {
+        if (PANELS) {
+            // SUMMA panels: C += acc as fire-and-forget L2 reductions, so the consumers go on with
+            // the next panel instead of waiting for C to load.  An FP64 atomic add rounds like
+            // the load-add-store it replaces; one thread owns each element, and its adds to one
+            // address stay in program order, so the panel order of the sums is kept.
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
+            for (int mt = 0; mt < 4; ++mt) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
-                if (row >= m_end) continue;
-                double *crow = dst_base + (size_t)row * ld;
+                for (int h = 0; h < 2; ++h) {
+                    const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
+                    if (row >= m_end) continue;
+                    double *crow = dst_base + (size_t)row * ld;
 #pragma unroll
-                for (int nt = 0; nt < 4; ++nt) {
-                    const int col = n0 + wn * 32 + nt * 8 + 2 * t;
-                    double v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-                    if (vec_store && col + 1 < n_end && col >= n_lo) {
-                        double2 *dst = reinterpret_cast<double2 *>(crow + col);
-                        if (beta_one) {
-                            const double2 old = *dst;
-                            v0 = old.x + v0;
-                            v1 = old.y + v1;
+                    for (int nt = 0; nt < 4; ++nt) {
+                        const int col = n0 + wn * 32 + nt * 8 + 2 * t;
+                        if (col < n_end && col >= n_lo)
+                            asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(crow + col),
+                                         "d"(acc[mt][nt][2 * h])
+                                         : "memory");
+                        if (col + 1 < n_end && col + 1 >= n_lo)
+                            asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(crow + col + 1),
+                                         "d"(acc[mt][nt][2 * h + 1])
+                                         : "memory");
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
+                    if (row >= m_end) continue;
+                    double *crow = dst_base + (size_t)row * ld;
+#pragma unroll
+                    for (int nt = 0; nt < 4; ++nt) {
+                        const int col = n0 + wn * 32 + nt * 8 + 2 * t;
+                        double v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
+                        if (vec_store && col + 1 < n_end && col >= n_lo) {
+                            double2 *dst = reinterpret_cast<double2 *>(crow + col);
+                            if (beta_one) {
+                                const double2 old = *dst;
+                                v0 = old.x + v0;
+                                v1 = old.y + v1;
+                            }
+                            *dst = make_double2(v0, v1);
+                        } else {
+                            if (col < n_end && col >= n_lo) crow[col] = beta_one ? crow[col] + v0 : v0;
+                            if (col + 1 < n_end && col + 1 >= n_lo)
+                                crow[col + 1] = beta_one ? crow[col + 1] + v1 : v1;
                         }
-                        *dst = make_double2(v0, v1);
-                    } else {
-                        if (col < n_end && col >= n_lo) crow[col] = beta_one ? crow[col] + v0 : v0;
-                        if (col + 1 < n_end && col + 1 >= n_lo) crow[col + 1] = beta_one ? crow[col + 1] + v1 : v1;
                     }
                 }
             }

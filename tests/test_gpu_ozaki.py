@@ -118,3 +118,9 @@ def test_host_buffer_entry_point_matches_device_path(mgx, oracle, form, panels, 
     else:
         mgx.gemm_fp64(dev(A), dev(B), dC)
     assert np.array_equal(bits(hC.numpy()), bits(host(dC)))
+    # the pool's cached scratch can be handed back, and the path allocates again afterwards
+    mgx.scratch_trim()
+    hC2 = torch.full((m, n), np.nan, dtype=torch.float64).pin_memory()
+    mgx.gemm_host(hA, hB, hC2, form=form, splits=8, panels=panels)
+    torch.cuda.synchronize()
+    assert np.array_equal(bits(hC2.numpy()), bits(hC.numpy()))
