@@ -47,12 +47,27 @@ def _mat(r, c, kind, seed, e_range=0):
 
 
 def cfg1():
+    """The drop-in call (mgx_ab_multiply, whole K per tile), then the FP64 tile shape the learned
+    cost model picks for this product (its K slices; 64 output tiles leave most SMs idle)."""
     n = 1024
     A, B, C = _mat(n, n, 1, 11), _mat(n, n, 1, 12), torch.empty((n, n), dtype=torch.float64, device="cuda")
     t = _time(lambda: mgx.ab_multiply(A, B, C), reps=20)
     e = mgx.error_vs_dd(A, B, C)
-    return {"config": "cfg1", "form": "fp64", "n": n, "tflops": 2 * n ** 3 / t / 1e12, "seconds": t,
-            "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "rows_checked": e["rows_checked"]}
+    out = [{"config": "cfg1", "form": "fp64", "n": n, "ksplit": 1, "tflops": 2 * n ** 3 / t / 1e12, "seconds": t,
+            "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "rows_checked": e["rows_checked"]}]
+    from mgxbench_b200 import autotune as at
+    from mgxbench_b200 import predictive as pr_mod
+    if pr_mod.DEFAULT_MODEL.is_file():
+        model = at.MlpModel.load(pr_mod.DEFAULT_MODEL)
+        fp64 = [c for c in at.candidates(n, n, n) if c.is_fp64]
+        c = at.choose(model, n, n, n, 0, 1.0, fp64)  # the form is fixed; the model picks the K slices
+        ws = mgx.OzakiWorkspace()
+        t2 = _time(lambda: mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws), reps=20)
+        e2 = mgx.error_vs_dd(A, B, C)
+        out.append({"config": "cfg1", "form": "fp64", "n": n, "ksplit": c.ksplit, "ksplit_from": "learned cost model",
+                    "tflops": 2 * n ** 3 / t2 / 1e12, "seconds": t2, "normwise_err": e2["normwise"],
+                    "max_rel_err": e2["max_rel"], "rows_checked": e2["rows_checked"]})
+    return out
 
 
 def cfg2():

@@ -381,18 +381,49 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
-// Split-K epilogue: C = (beta ? C : 0) + slice 0 + slice 1 + ... in that fixed order, so the
-// result does not depend on which CTA finished first.
+// Split-K epilogue: C = (beta ? C : 0) + (slice 0 + slice 1 + ...), the slices summed in that
+// fixed order, so the result does not depend on which CTA finished first.  Two columns per
+// thread: the partial rows are 16-byte aligned (even ld, 256-byte aligned base; the pad column
+// of an odd n is read and dropped).
 __global__ void splitk_reduce(double *__restrict__ C, int ldc, int beta_one, const double *__restrict__ P, int ld,
                               size_t stride, int slices, int m, int n)
 {
+    const bool c_vec = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
     for (int row = blockIdx.x; row < m; row += gridDim.x) {
-        for (int col = threadIdx.x; col < n; col += blockDim.x) {
-            const size_t o = (size_t)row * ld + col;
-            double v = P[o];
-            for (int s = 1; s < slices; ++s) v += P[o + (size_t)s * stride];
-            double *c = C + (size_t)row * ldc + col;
-            *c = beta_one ? *c + v : v;
+        const double *prow = P + (size_t)row * ld;
+        double *crow = C + (size_t)row * ldc;
+        for (int col = 2 * threadIdx.x; col < n; col += 2 * blockDim.x) {
+            double2 v = *reinterpret_cast<const double2 *>(prow + col);
+            int s = 1;
+            for (; s + 3 < slices; s += 4) {  // four independent loads in flight, summed in order
+                const double2 p1 = *reinterpret_cast<const double2 *>(prow + (size_t)s * stride + col);
+                const double2 p2 = *reinterpret_cast<const double2 *>(prow + (size_t)(s + 1) * stride + col);
+                const double2 p3 = *reinterpret_cast<const double2 *>(prow + (size_t)(s + 2) * stride + col);
+                const double2 p4 = *reinterpret_cast<const double2 *>(prow + (size_t)(s + 3) * stride + col);
+                v.x = (((v.x + p1.x) + p2.x) + p3.x) + p4.x;
+                v.y = (((v.y + p1.y) + p2.y) + p3.y) + p4.y;
+            }
+            for (; s < slices; ++s) {
+                const double2 p1 = *reinterpret_cast<const double2 *>(prow + (size_t)s * stride + col);
+                v.x += p1.x;
+                v.y += p1.y;
+            }
+            if (col + 1 < n) {
+                if (c_vec) {
+                    double2 *dst = reinterpret_cast<double2 *>(crow + col);
+                    if (beta_one) {
+                        const double2 o = *dst;
+                        v.x = o.x + v.x;
+                        v.y = o.y + v.y;
+                    }
+                    *dst = v;
+                } else {
+                    crow[col] = beta_one ? crow[col] + v.x : v.x;
+                    crow[col + 1] = beta_one ? crow[col + 1] + v.y : v.y;
+                }
+            } else {
+                crow[col] = beta_one ? crow[col] + v.x : v.x;
+            }
         }
     }
 }

@@ -148,16 +148,22 @@ __global__ void ozaki_col_exp(const unsigned long long *__restrict__ colmax, int
     }
 }
 
-// Digits of one value (same operations as the oracle's digits_of).
+// Digits of one value (the oracle's digits_of: d = rint(x), x <- (x - d) * 128).  rint is
+// computed by adding 1.5 * 2^52: for |x| < 2^51 the sum is rounded to an integer by the add
+// itself, to nearest with ties to even (as rint), and the integer sits in the low bits of the
+// sum.  Subtracting the constant back gives rint(x) exactly.  Two full-rate adds replace a
+// round and a float-to-int conversion per digit.
 template <int S>
 __device__ __forceinline__ void digits(double v, int e, int8_t (&d)[S], int s)
 {
+    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
     double x = scale2(v, 6 - e);
 #pragma unroll
     for (int t = 0; t < S; ++t) {
         if (t < s) {
-            const double r = rint(x);
-            d[t] = (int8_t)(int)r;
+            const double y = __dadd_rn(x, kRound);
+            const double r = __dsub_rn(y, kRound);
+            d[t] = (int8_t)__double2loint(y);
             x = (x - r) * 128.0;
         } else {
             d[t] = 0;

@@ -90,3 +90,27 @@ def test_trained_network_beats_regression_on_measured_sweep():
     assert em["regret"]["1e-15"]["mean_regret"] < er["regret"]["1e-15"]["mean_regret"]
     assert em["mean_regret_over_targets"] < er["mean_regret_over_targets"]
     assert em["accuracy"]["runtime_abs_ln_median"] < er["accuracy"]["runtime_abs_ln_median"]
+
+
+def test_predictive_auto_validates_through_the_executable(tmp_path):
+    """MGXBench-shaped AUTO with --auto-validate --auto-feedback: the packaged model's choice is run
+    by build/mm_1d and the measurement is appended to a sweep database."""
+    import shutil
+    import types
+
+    from mgxbench_b200 import predictive as pr
+    if not (DATA / "mlp_b200.json").is_file():
+        pytest.skip("no packaged model")
+    db = tmp_path / "db.jsonl"
+    shutil.copy(DATA / "sweep_b200.jsonl", db)
+    n_before = len(db.read_text().splitlines())
+    args = types.SimpleNamespace(decomposition="1d", ranks=2, size=2048, grid_rows=None, grid_cols=None,
+                                 prediction_model="ml", auto_model=None, db=str(db), auto_validate=True,
+                                 auto_feedback=True, build_dir="build", output=str(tmp_path / "out"), warmup=1,
+                                 repeats=2, timeout=300, exp_range=10, target=1e-15, project_root=str(ROOT))
+    assert pr.auto(args) == 0
+    rep = json.loads((tmp_path / "out" / "autotuning_prediction.json").read_text())
+    assert rep["status"] == "VALIDATED" and rep["measured"] is True
+    assert rep["validation"]["measured_s"] > 0 and rep["validation"]["valid"] is True
+    assert rep["feedback"]["status"] == "SAVED"
+    assert len(db.read_text().splitlines()) == n_before + 1
