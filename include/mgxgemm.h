@@ -132,6 +132,18 @@ MGX_API int mgx_gemm_ozaki(const double *A, const double *B, double *C, int m, i
                            int ldc, int beta_one, int splits, void *workspace, size_t workspace_bytes,
                            void *stream);
 
+/* Split-K form of mgx_gemm_ozaki for products with few 128 x 128 output tiles (small m n, long
+ * k): the 32-wide K blocks are cut into `ksplit` slices computed by separate CTAs; each slice's
+ * group sums are recombined and scaled on their own, and the slice results are added into C in
+ * slice order (deterministic).  The exponents and digits are those of the whole K range, so only
+ * the final additions differ from mgx_gemm_ozaki.  Needs k <= mgx_ozaki_kmax(splits) and
+ * mgx_ozaki_splitk_workspace_size(m, n, k, splits, ksplit) bytes of 256-byte aligned workspace
+ * (0 when k is too long).  No counterpart in MGXBench; the autotuner picks ksplit. */
+MGX_API size_t mgx_ozaki_splitk_workspace_size(int m, int n, int k, int splits, int ksplit);
+MGX_API int mgx_gemm_ozaki_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                  int ldb, int ldc, int beta_one, int splits, int ksplit, void *workspace,
+                                  size_t workspace_bytes, void *stream);
+
 /* The two phases of mgx_gemm_ozaki for one K range of at most mgx_ozaki_kmax(splits):
  * mgx_ozaki_split writes the exponents and digit slices of A and B into the workspace;
  * mgx_ozaki_multiply runs the INT8 tensor-core products and the FP64 recombination into C.

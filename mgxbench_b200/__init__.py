@@ -65,6 +65,8 @@ EXPORTS = [
     ("mgx_gemm_fp64_splitk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_ozaki", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_ozaki_splitk_workspace_size", _sz, [_i, _i, _i, _i, _i]),
+    ("mgx_gemm_ozaki_splitk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_choose_splits", _i, [_i, _d, _d]),
     ("mgx_ozaki_split", _i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_multiply", _i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
@@ -209,10 +211,22 @@ class OzakiWorkspace:
 _default_ws = OzakiWorkspace()
 
 
-def gemm_ozaki(A, B, C, splits: int = 8, beta_one: bool = False, workspace=None, stream=None):
+def ozaki_splitk_workspace_size(m, n, k, splits, ksplit) -> int:
+    return int(lib().mgx_ozaki_splitk_workspace_size(m, n, k, splits, ksplit))
+
+
+def gemm_ozaki(A, B, C, splits: int = 8, beta_one: bool = False, workspace=None, stream=None, ksplit: int = 1):
+    """C (+)= A B by the Ozaki form; ksplit > 1 cuts K into slices computed by separate CTAs
+    (mgx_gemm_ozaki_splitk, for products with few output tiles)."""
     _check_f64(A, B, C)
     m, k = A.shape
     n = B.shape[1]
+    if ksplit > 1:
+        need = ozaki_splitk_workspace_size(m, n, k, splits, ksplit)
+        ws = (workspace or _default_ws).get(need)
+        return _check(lib().mgx_gemm_ozaki_splitk(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
+                                                  int(beta_one), splits, ksplit, _ptr(ws), ws.numel(),
+                                                  _stream(stream)), "mgx_gemm_ozaki_splitk")
     need = ozaki_workspace_size(m, n, k, splits)
     ws = (workspace or _default_ws).get(need)
     return _check(lib().mgx_gemm_ozaki(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),

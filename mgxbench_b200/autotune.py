@@ -30,10 +30,13 @@ from pathlib import Path
 import numpy as np
 
 TILE_FP64 = 0          # native FP64 kernel (DMMA), 128 x 128 output tiles over the whole K range
-TILE_OZAKI_128 = 1     # Ozaki INT8 kernel, 128 x 128 output tiles
+TILE_OZAKI_128 = 1     # Ozaki INT8 kernel, 128 x 128 output tiles over the whole K range
 # native FP64 kernel, 128 x 128 output tiles, K cut into 2 / 4 / 8 / 16 slices (split-K)
 TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16 = 2, 3, 4, 5
+# Ozaki INT8 kernel, 128 x 128 output tiles, K cut into 4 / 16 slices (split-K)
+TILE_OZAKI_K4, TILE_OZAKI_K16 = 6, 7
 FP64_KSPLIT = {TILE_FP64: 1, TILE_FP64_K2: 2, TILE_FP64_K4: 4, TILE_FP64_K8: 8, TILE_FP64_K16: 16}
+OZAKI_KSPLIT = {TILE_OZAKI_128: 1, TILE_OZAKI_K4: 4, TILE_OZAKI_K16: 16}
 SPLITS = tuple(range(3, 10))
 ERROR_FLOOR = 1e-17
 
@@ -49,30 +52,40 @@ class Candidate:
 
     @property
     def ksplit(self) -> int:
-        return FP64_KSPLIT.get(self.tile, 1)
+        return FP64_KSPLIT.get(self.tile) or OZAKI_KSPLIT.get(self.tile, 1)
 
     @property
     def name(self) -> str:
-        if self.is_fp64:
-            return "fp64" if self.ksplit == 1 else f"fp64k{self.ksplit}"
-        return f"ozaki{self.splits}"
+        base = "fp64" if self.is_fp64 else f"ozaki{self.splits}"
+        return base if self.ksplit == 1 else f"{base}k{self.ksplit}"
 
 
 SPLITK_WORKSPACE_LIMIT = 4 << 30   # bytes of split-K partial products a candidate may need
 
 
-def splitk_applies(m, n, k, ksplit):
+def ozaki_kmax(s):
+    """Longest K one int32 accumulation of s-digit slice products takes (mgx_ozaki_kmax)."""
+    return (2147483647 // (4096 * s)) & ~127
+
+
+def splitk_applies(m, n, k, ksplit, splits=0):
     """A split-K candidate is offered when every slice gets a 32-wide K block and the partial
-    products fit SPLITK_WORKSPACE_LIMIT (the executables apply the same rule)."""
-    return ksplit == 1 or ((k + 31) // 32 >= ksplit and ksplit * m * n * 8 <= SPLITK_WORKSPACE_LIMIT)
+    products fit SPLITK_WORKSPACE_LIMIT; an Ozaki one also needs K within one int32 accumulation
+    (the executables apply the same rule)."""
+    if ksplit == 1:
+        return True
+    if splits and k > ozaki_kmax(splits):
+        return False
+    return (k + 31) // 32 >= ksplit and ksplit * m * n * 8 <= SPLITK_WORKSPACE_LIMIT
 
 
 def candidates(m=None, n=None, k=None):
     """Every configuration, or those that apply to an m x n x k product."""
-    fp64 = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16)]
+    out = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16)]
+    out += [Candidate(t, s) for t in (TILE_OZAKI_128, TILE_OZAKI_K4, TILE_OZAKI_K16) for s in SPLITS]
     if m is not None:
-        fp64 = [c for c in fp64 if splitk_applies(m, n, k, c.ksplit)]
-    return fp64 + [Candidate(TILE_OZAKI_128, s) for s in SPLITS]
+        out = [c for c in out if splitk_applies(m, n, k, c.ksplit, c.splits)]
+    return out
 
 
 def features(m, n, k, exp_range, cand: Candidate):
@@ -102,7 +115,7 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
             if c.is_fp64:
                 mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws)
             else:
-                mgx.gemm_ozaki(A, B, C, splits=c.splits, workspace=ws)
+                mgx.gemm_ozaki(A, B, C, splits=c.splits, workspace=ws, ksplit=c.ksplit)
         run()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -112,7 +125,7 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
         e1.record()
         e1.synchronize()
         t = e0.elapsed_time(e1) / reps * 1e-3
-        key = (c.ksplit, c.splits)  # Ozaki results do not depend on the tile; FP64 ones on the K slices
+        key = (c.is_fp64, c.ksplit, c.splits)  # results depend on the form, K slices and split count only
         if key not in errors:
             rows = min(check_rows, m)
             errors[key] = mgx.error_vs_dd(A, B, C, row_start=(m - rows) // 2, row_count=rows)["normwise"]

@@ -460,6 +460,18 @@ static void splitk_geometry(int k_len, int ksplit, int *kb_split, int *slices)
     *slices = *kb_split > 0 ? (kblocks + *kb_split - 1) / *kb_split : 1;
 }
 
+// Launches the split-K epilogue (also used by the Ozaki form's split-K).
+int mgx_launch_splitk_reduce(double *C, int ldc, int beta_one, const double *P, int ld, size_t stride, int slices,
+                             int m, int n, cudaStream_t stream)
+{
+    if (m <= 0 || n <= 0) return MGX_SUCCESS;
+    int rgrid = mgx_sm_count() * 8;
+    if (rgrid > m) rgrid = m;
+    fp64::splitk_reduce<<<rgrid, 256, 0, stream>>>(C, ldc, beta_one, P, ld, stride, slices, m, n);
+    MGX_HOST_CHECK(cudaGetLastError());
+    return MGX_SUCCESS;
+}
+
 size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit)
 {
     int kbs, slices;

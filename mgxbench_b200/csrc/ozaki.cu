@@ -64,6 +64,11 @@ struct GemmParams {
     int beta_one;
     int vec_store;
     int *status;
+    int ksplit;               // > 1: work item w is (tile w / ksplit, K slice w % ksplit)
+    int kb_split;             // K blocks per slice
+    double *partial;          // split-K: slice s's scaled result goes to partial + s * partial_stride
+    int partial_ld;           // even
+    size_t partial_stride;
 };
 
 // ---------------------------------------------------------------- shared numerics
@@ -318,6 +323,16 @@ __device__ __forceinline__ void tile_of(const GemmParams &p, int w, int &m0, int
     n0 = (r / gsize) * TILE;
 }
 
+// Work item w: its output tile (8-tile-row raster over the tiles) and its K blocks
+// [kb_begin, kb_end) -- all of K, or one slice of it in the split-K form.
+__device__ __forceinline__ void item_of(const GemmParams &p, int w, int &m0, int &n0, int &kb_begin, int &kb_end)
+{
+    const int ks = p.ksplit > 1 ? p.ksplit : 1;
+    tile_of(p, w / ks, m0, n0);
+    kb_begin = (w % ks) * p.kb_split;
+    kb_end = min(p.kblocks, kb_begin + p.kb_split);
+}
+
 // Weight sets of up to four consecutive groups, highest weights first (the same rule as the
 // host's, at compile time so the MMA issue sequence can be unrolled completely).
 __host__ __device__ constexpr int set_lo_of(int dhi) { return (dhi - 3 > 2) ? dhi - 3 : 2; }
@@ -374,18 +389,18 @@ __device__ __forceinline__ void issue_stage(uint32_t tmem_base, uint64_t a0, uin
 template <int S, int SI>
 __device__ __forceinline__ bool mma_set(const GemmParams &p, uint32_t smem_base, uint32_t tmem_base, uint64_t *full,
                                         uint64_t *empty, uint64_t *acc_full, uint64_t *acc_empty, int &stage,
-                                        uint32_t &phase, uint32_t &acc_phase)
+                                        uint32_t &phase, uint32_t &acc_phase, int kb_begin, int kb_end)
 {
     constexpr int DHI = set_hi(S, SI), NSL = cmin(S, DHI - 1), KPACK = S / NSL;
     if (!mbar_wait_bounded(acc_empty, acc_phase ^ 1u, p.status, kDevTimeoutAcc)) return false;
     acc_phase ^= 1u;
     tc_fence_after();
-    for (int kb0 = 0; kb0 < p.kblocks; kb0 += KPACK) {
+    for (int kb0 = kb_begin; kb0 < kb_end; kb0 += KPACK) {
         if (!mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull)) return false;
         tc_fence_after();
         const uint32_t sa = smem_base + stage * p.stage_bytes;
-        issue_stage<S, SI>(tmem_base, sw32_desc(sa), sw32_desc(sa + S * SLICE_TILE_BYTES), min(KPACK, p.kblocks - kb0),
-                           kb0 == 0);
+        issue_stage<S, SI>(tmem_base, sw32_desc(sa), sw32_desc(sa + S * SLICE_TILE_BYTES), min(KPACK, kb_end - kb0),
+                           kb0 == kb_begin);
         tc_commit(&empty[stage]);  // frees the stage once these MMAs have read it
         if (++stage == p.stages) {
             stage = 0;
@@ -411,6 +426,7 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = ((p.m + TILE - 1) / TILE) * ((p.n + TILE - 1) / TILE);
+    const int items = total * (p.ksplit > 1 ? p.ksplit : 1);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < p.stages; ++s) {
@@ -441,21 +457,21 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
             int armed[4] = {-1, -1, -1, -1};
             bool ok = true;
             const size_t slab = (size_t)p.splits * SLICE_TILE_BYTES;  // all slices of one 128-row tile, one K block
-            for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
-                int m0, n0;
-                tile_of(p, w, m0, n0);
+            for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
+                int m0, n0, kb_begin, kb_end;
+                item_of(p, w, m0, n0, kb_begin, kb_end);
                 const uint8_t *ga = p.da + (size_t)(m0 / TILE) * p.kblocks * slab;
                 const uint8_t *gb = p.db + (size_t)(n0 / TILE) * p.kblocks * slab;
                 for (int si = 0; si < p.num_sets && ok; ++si) {
                     const int nsl = min(p.splits, p.set_dhi[si] - 1);
                     const int kpack = p.splits / nsl;   // K blocks per stage: every stage ~2s tiles
                     const uint32_t bytes = (uint32_t)(nsl * SLICE_TILE_BYTES);
-                    for (int kb0 = 0; kb0 < p.kblocks; kb0 += kpack) {
+                    for (int kb0 = kb_begin; kb0 < kb_end; kb0 += kpack) {
                         if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty)) {
                             ok = false;
                             break;
                         }
-                        const int nkb = min(kpack, p.kblocks - kb0);
+                        const int nkb = min(kpack, kb_end - kb0);
                         unsigned char *sa = smem + stage * p.stage_bytes;
                         unsigned char *sb = sa + p.splits * SLICE_TILE_BYTES;
                         mbar_arrive_expect_tx(&full[stage], 2u * (uint32_t)nkb * bytes);
@@ -467,7 +483,7 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
                         }
                         // warm L2 with the slabs this CTA will copy PREFETCH_STAGES stages from now
                         const int kbp = kb0 + PREFETCH_STAGES * kpack;
-                        for (int j = 0; j < kpack && kbp + j < p.kblocks; ++j) {
+                        for (int j = 0; j < kpack && kbp + j < kb_end; ++j) {
                             bulk_prefetch_l2(ga + (size_t)(kbp + j) * slab, bytes);
                             bulk_prefetch_l2(gb + (size_t)(kbp + j) * slab, bytes);
                         }
@@ -489,14 +505,17 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
             bool ok = true;
             const uint32_t smem_base = smem_u32(smem);
             constexpr int NS = num_sets_of(S);
-            for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
-                ok = mma_set<S, 0>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage, phase, acc_phase);
+            for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
+                int m0, n0, kb_begin, kb_end;
+                item_of(p, w, m0, n0, kb_begin, kb_end);
+                ok = mma_set<S, 0>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage, phase, acc_phase,
+                                   kb_begin, kb_end);
                 if (NS > 1 && ok)
                     ok = mma_set<S, (NS > 1 ? 1 : 0)>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage,
-                                                      phase, acc_phase);
+                                                      phase, acc_phase, kb_begin, kb_end);
                 if (NS > 2 && ok)
                     ok = mma_set<S, (NS > 2 ? 2 : 0)>(p, smem_base, tmem_base, full, empty, acc_full, acc_empty, stage,
-                                                      phase, acc_phase);
+                                                      phase, acc_phase, kb_begin, kb_end);
             }
             // Drain: all MMAs this thread issued have finished before TMEM is released.
             tc_commit(drain);
@@ -508,10 +527,16 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
         const int half = (warp - 2) >> 2;   // which 64 of the 128 columns
         uint32_t acc_phase = 0;
         bool ok = true;
-        for (int w = blockIdx.x; w < total && ok; w += gridDim.x) {
-            int m0, n0;
-            tile_of(p, w, m0, n0);
+        for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
+            int m0, n0, kb_begin, kb_end;
+            item_of(p, w, m0, n0, kb_begin, kb_end);
             const int m_end = p.m, n_end = p.n;
+            // destination: C, or this K slice's partial results (plain stores, summed later)
+            const bool split = p.ksplit > 1;
+            double *const dbase = split ? p.partial + (size_t)(w % p.ksplit) * p.partial_stride : p.C;
+            const int dld = split ? p.partial_ld : p.ldc;
+            const int dvec = split ? 1 : p.vec_store;
+            const int dbeta = split ? 0 : p.beta_one;
             double h[64];
 #pragma unroll
             for (int j = 0; j < 64; ++j) h[j] = 0.0;
@@ -546,7 +571,7 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
             const int row = m0 + 32 * q + lane;
             if (row < m_end) {
                 const int er = p.ea[row];
-                double *crow = p.C + (size_t)row * p.ldc;
+                double *crow = dbase + (size_t)row * dld;
                 const int cbase = n0 + half * 64;
 #pragma unroll
                 for (int j = 0; j < 64; j += 2) {
@@ -560,20 +585,20 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
                         double v1 = (er == NONFINITE_EXP || e1 == NONFINITE_EXP)
                                         ? __longlong_as_double(0x7ff8000000000000ll)
                                         : scale2(h[j + 1], er + e1 - 12);
-                        if (p.vec_store) {
+                        if (dvec) {
                             double2 *dst = reinterpret_cast<double2 *>(crow + col);
-                            if (p.beta_one) {
+                            if (dbeta) {
                                 const double2 o = *dst;
                                 v0 = o.x + v0;
                                 v1 = o.y + v1;
                             }
                             *dst = make_double2(v0, v1);
                         } else {
-                            crow[col] = p.beta_one ? crow[col] + v0 : v0;
-                            crow[col + 1] = p.beta_one ? crow[col + 1] + v1 : v1;
+                            crow[col] = dbeta ? crow[col] + v0 : v0;
+                            crow[col + 1] = dbeta ? crow[col + 1] + v1 : v1;
                         }
                     } else {
-                        crow[col] = p.beta_one ? crow[col] + v0 : v0;
+                        crow[col] = dbeta ? crow[col] + v0 : v0;
                     }
                 }
             }
@@ -717,8 +742,30 @@ static int ozaki_split_impl(const double *A, const double *B, int m, int n, int 
 }
 
 // Phase 2: C (+)= recombined slice products (tcgen05 kernel).
+int mgx_launch_splitk_reduce(double *C, int ldc, int beta_one, const double *P, int ld, size_t stride, int slices,
+                             int m, int n, cudaStream_t stream);
+
+// Split-K geometry of the Ozaki kernel (the FP64 kernel's rule): K blocks per slice and the
+// number of non-empty slices.
+static void ozaki_splitk_geometry(int k, int ksplit, int *kb_split, int *slices)
+{
+    const int kblocks = (k + 31) / 32 > 0 ? (k + 31) / 32 : 1;
+    if (ksplit < 1) ksplit = 1;
+    if (ksplit > kblocks) ksplit = kblocks;
+    *kb_split = (kblocks + ksplit - 1) / ksplit;
+    *slices = (kblocks + *kb_split - 1) / *kb_split;
+}
+
+static size_t ozaki_partial_bytes(int m, int n, int k, int ksplit)
+{
+    int kbs, slices;
+    ozaki_splitk_geometry(k, ksplit, &kbs, &slices);
+    if (slices <= 1 || m <= 0 || n <= 0) return 0;
+    return align256((size_t)slices * (size_t)m * (size_t)((n + 1) & ~1) * sizeof(double));
+}
+
 static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta_one, int s, const unsigned char *ws,
-                               const WsLayout &L, cudaStream_t stream)
+                               const WsLayout &L, cudaStream_t stream, int ksplit = 1, double *partial = nullptr)
 {
     oz::GemmParams p;
     memset(&p, 0, sizeof p);
@@ -751,9 +798,20 @@ static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta
     p.db = ws + L.db;
     p.beta_one = beta_one;
     p.vec_store = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+    int kb_split = p.kblocks, slices = 1;
+    if (ksplit > 1) ozaki_splitk_geometry(k, ksplit, &kb_split, &slices);
+    p.ksplit = slices;
+    p.kb_split = kb_split;
+    p.partial = slices > 1 ? partial : nullptr;
+    p.partial_ld = (n + 1) & ~1;
+    p.partial_stride = (size_t)m * (size_t)p.partial_ld;
+    if (slices > 1 && (!partial || (reinterpret_cast<uintptr_t>(partial) & 255))) {
+        mgx_set_last_message("mgx_gemm_ozaki_splitk: no 256-byte aligned partial-product buffer");
+        return MGX_E_WORKSPACE;
+    }
     p.status = mgx_device_status_ptr();
     const int smem = p.stages * p.stage_bytes + 1024 + 256;
-    const int total = ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE);
+    const int total = ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE) * slices;
     const int sms = mgx_sm_count();
     const int grid = sms < total ? sms : total;
     if (grid < 1) return MGX_SUCCESS;
@@ -761,6 +819,9 @@ static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta
         MGX_HOST_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         kernel<<<grid, oz::THREADS, smem, stream>>>(p);
         MGX_HOST_CHECK(cudaGetLastError());
+        if (slices > 1)  // C (+)= slice 0 + slice 1 + ..., in slice order
+            return mgx_launch_splitk_reduce(C, ldc, beta_one, partial, p.partial_ld, p.partial_stride, slices, m, n,
+                                            stream);
         return MGX_SUCCESS;
     };
     switch (s) {
@@ -837,6 +898,46 @@ extern "C" MGX_API int mgx_gemm_ozaki(const double *A, const double *B, double *
 {
     return mgx_ozaki_run(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, splits, workspace, workspace_bytes,
                          (cudaStream_t)stream);
+}
+
+extern "C" MGX_API size_t mgx_ozaki_splitk_workspace_size(int m, int n, int k, int splits, int ksplit)
+{
+    if (m < 0 || n < 0 || k < 0 || splits < 2 || splits > oz::MAX_SPLITS || ksplit < 1) return 0;
+    if (k > ozaki_kmax(splits)) return 0;
+    return ws_layout(m, n, k, splits).total + ozaki_partial_bytes(m, n, k, ksplit);
+}
+
+extern "C" MGX_API int mgx_gemm_ozaki_splitk(const double *A, const double *B, double *C, int m, int n, int k,
+                                             int lda, int ldb, int ldc, int beta_one, int splits, int ksplit,
+                                             void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!ozaki_args_ok(m, n, k, splits) || ksplit < 1 || (m > 0 && n > 0 && !C) ||
+        (m > 0 && n > 0 && k > 0 && (!A || !B || lda < k || ldb < n)) || (m > 0 && n > 0 && ldc < n)) {
+        mgx_set_last_message("mgx_gemm_ozaki_splitk: invalid arguments m=%d n=%d k=%d splits=%d ksplit=%d", m, n, k,
+                             splits, ksplit);
+        return MGX_E_INVALID;
+    }
+    if (k > ozaki_kmax(splits)) {
+        mgx_set_last_message("mgx_gemm_ozaki_splitk: k = %d is above one int32 accumulation (%d) for %d splits", k,
+                             ozaki_kmax(splits), splits);
+        return MGX_E_UNSUPPORTED;
+    }
+    if (ksplit == 1 || m == 0 || n == 0 || k == 0)
+        return mgx_ozaki_run(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, splits, workspace, workspace_bytes,
+                             (cudaStream_t)stream);
+    const WsLayout L = ws_layout(m, n, k, splits);
+    const size_t need = L.total + ozaki_partial_bytes(m, n, k, ksplit);
+    if (!workspace || workspace_bytes < need || (reinterpret_cast<uintptr_t>(workspace) & 255)) {
+        mgx_set_last_message("mgx_gemm_ozaki_splitk: workspace of %zu bytes (aligned to 256) needed, %zu given", need,
+                             workspace_bytes);
+        return MGX_E_WORKSPACE;
+    }
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ozaki_split_impl(A, B, m, n, k, lda, ldb, splits, ws, L, st);
+    if (rc != MGX_SUCCESS) return rc;
+    return ozaki_multiply_impl(C, m, n, k, ldc, beta_one ? 1 : 0, splits, ws, L, st, ksplit,
+                               reinterpret_cast<double *>(ws + L.total));
 }
 
 // A-priori split choice.  The normwise error of the Ozaki form falls by close to two decimal

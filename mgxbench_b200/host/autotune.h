@@ -79,8 +79,8 @@ inline std::string exe_dir()
 
 inline std::string default_model_path() { return exe_dir() + "/../mgxbench_b200/data/mlp_b200.json"; }
 
-// Tile ids of the candidates (mgxbench_b200.autotune): 1 is the Ozaki kernel; 0, 2, 3, 4, 5 are
-// the FP64 kernel with the K range cut into 1, 2, 4, 8, 16 slices.
+// Tile ids of the candidates (mgxbench_b200.autotune): 0, 2, 3, 4, 5 are the FP64 kernel with
+// the K range cut into 1, 2, 4, 8, 16 slices; 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices.
 inline int tile_ksplit(int tile)
 {
     switch (tile) {
@@ -88,17 +88,21 @@ inline int tile_ksplit(int tile)
     case 3: return 4;
     case 4: return 8;
     case 5: return 16;
+    case 6: return 4;
+    case 7: return 16;
     default: return 1;
     }
 }
 
-inline bool tile_is_fp64(int tile) { return tile != 1; }
+inline bool tile_is_fp64(int tile) { return tile != 1 && tile != 6 && tile != 7; }
 
-// Same rule as mgxbench_b200.autotune.splitk_applies: each slice gets a 32-wide K block and the
-// partial products fit 4 GiB.
-inline bool splitk_applies(int m, int n, int k, int ksplit)
+// Same rule as mgxbench_b200.autotune.splitk_applies: each slice gets a 32-wide K block, the
+// partial products fit 4 GiB, and an Ozaki split needs K within one int32 accumulation.
+inline bool splitk_applies(int m, int n, int k, int ksplit, int splits)
 {
-    return ksplit == 1 || ((k + 31) / 32 >= ksplit && (double)ksplit * m * n * 8.0 <= 4294967296.0);
+    if (ksplit == 1) return true;
+    if (splits > 0 && k > mgx_ozaki_kmax(splits)) return false;
+    return (k + 31) / 32 >= ksplit && (double)ksplit * m * n * 8.0 <= 4294967296.0;
 }
 
 // Loads the model at `path` and picks the form and split count for an m x n x k product whose
@@ -128,16 +132,17 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
     }
     if (!json_numbers(text, "candidates", &cand) || cand.empty() || cand.size() % 2) {
         cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0};  // default list: FP64 (1..16 K slices), Ozaki 3..9 splits
-        for (int s = 3; s <= 9; ++s) {
-            cand.push_back(1);
-            cand.push_back(s);
-        }
+        for (int t : {1, 6, 7})                 // with 1, 4, 16 K slices
+            for (int s = 3; s <= 9; ++s) {
+                cand.push_back(t);
+                cand.push_back(s);
+            }
     }
     {   // keep the candidates that apply to this product
         std::vector<double> keep;
         for (size_t c = 0; c + 1 < cand.size(); c += 2) {
-            const int ks = tile_is_fp64((int)cand[c]) ? tile_ksplit((int)cand[c]) : 1;
-            if (!splitk_applies(m, n, k, ks) || (whole_k_only && ks > 1)) continue;
+            const int ks = tile_ksplit((int)cand[c]);
+            if (!splitk_applies(m, n, k, ks, (int)cand[c + 1]) || (whole_k_only && ks > 1)) continue;
             keep.push_back(cand[c]);
             keep.push_back(cand[c + 1]);
         }
@@ -193,7 +198,7 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
     const int pick = best >= 0 ? best : most;
     out->form = tile_is_fp64((int)cand[2 * pick]) ? MGX_FORM_FP64 : MGX_FORM_OZAKI;
     out->splits = (int)cand[2 * pick + 1];
-    out->ksplit = tile_is_fp64((int)cand[2 * pick]) ? tile_ksplit((int)cand[2 * pick]) : 1;
+    out->ksplit = tile_ksplit((int)cand[2 * pick]);
     out->predicted_s = std::exp(Y[(size_t)pick * 2] * ystd[0] + ymean[0]);
     out->predicted_err = std::pow(10.0, Y[(size_t)pick * 2 + 1] * ystd[1] + ymean[1]);
     out->model_path = path;

@@ -86,7 +86,7 @@ int main(int argc, char *argv[])
     // the choice is made for the product each emulated rank runs (its K chunk when chunked)
     mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, mi, n, chunked ? std::min(pipeline_k_chunk, k) : k,
                           input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, EXIT_FAILURE, chunked);
-    if (chunked || form != mm::kFp64) ksplit = 1;
+    if (chunked) ksplit = 1;
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
     printf("mmb one-GPU emulation: ranks=%d rows/rank=%d form=%s%s input=%s B-structure=%s", nRanks, mi,
            form_name.c_str(), form == mm::kOzaki ? (std::string(" splits=") + std::to_string(splits)).c_str() : "",

@@ -112,7 +112,7 @@ struct Workspace {
     }
 };
 
-// One block multiply C (+)= A B of the selected form (FP64 with `ksplit` K slices).
+// One block multiply C (+)= A B of the selected form with `ksplit` K slices.
 inline int block_gemm(int form, int splits, int ksplit, Workspace &ws, const double *A, const double *B, double *C,
                       int m, int n, int k, int lda, int ldb, int ldc, int beta_one, cudaStream_t s)
 {
@@ -123,6 +123,12 @@ inline int block_gemm(int form, int splits, int ksplit, Workspace &ws, const dou
         return mgx_gemm_fp64_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one, ksplit, w, need, s);
     }
     if (form == kFp64) return mgx_gemm_fp64(A, B, C, m, n, k, lda, ldb, ldc, beta_one, s);
+    if (ksplit > 1) {
+        const size_t need = mgx_ozaki_splitk_workspace_size(m, n, k, splits, ksplit);
+        void *w = ws.get(need);
+        if (!w && need) return MGX_E_CUDA;
+        return mgx_gemm_ozaki_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one, splits, ksplit, w, need, s);
+    }
     const size_t need = mgx_ozaki_workspace_size(m, n, k, splits);
     void *w = ws.get(need);
     if (!w && need) return MGX_E_CUDA;

@@ -626,5 +626,64 @@ ORACLE_API int oracle_ozaki_gemm(const double *A, const double *B, double *C, in
     return 0;
 }
 
+/* Split-K form of the Ozaki product (k <= oracle_ozaki_kmax(s)), as the GPU computes it: the
+ * exponents and digits come from the whole K range; the 32-wide K blocks are cut into slices of
+ * ceil(kblocks / ksplit) blocks; each slice's group sums are recombined (Horner) and scaled on
+ * their own, and the slice results are added in slice order:
+ *   v = P_0 + P_1 + ... (left to right);  C = beta_one ? C + v : v.
+ * With one slice this is oracle_ozaki_gemm.  Returns 1 on non-finite input, 2 if k > kmax. */
+ORACLE_API int oracle_ozaki_gemm_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                        int ldb, int ldc, int s, int ksplit, int beta_one, int nthreads)
+{
+    nthreads = pick_threads(nthreads);
+    if (k > (oracle_ozaki_kmax(s) & ~127)) return 2;
+    const int kblocks = (k + 31) / 32 > 0 ? (k + 31) / 32 : 1;
+    if (ksplit < 1) ksplit = 1;
+    if (ksplit > kblocks) ksplit = kblocks;
+    const int kbs = (kblocks + ksplit - 1) / ksplit;
+    const int slices = (kblocks + kbs - 1) / kbs;
+    int32_t *ea = (int32_t *)malloc(sizeof(int32_t) * (m > 0 ? m : 1));
+    int32_t *eb = (int32_t *)malloc(sizeof(int32_t) * (n > 0 ? n : 1));
+    if (oracle_ozaki_exponents(A, B, m, n, k, lda, ldb, ea, eb)) {
+        free(ea);
+        free(eb);
+        return 1;
+    }
+    const int kp = (k + 15) & ~15;
+    int8_t *da = (int8_t *)malloc((size_t)s * m * kp + 1);
+    int8_t *db = (int8_t *)malloc((size_t)s * n * kp + 1);
+    oracle_ozaki_split(A, B, m, n, k, lda, ldb, s, kp, ea, eb, da, db);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+    for (int i = 0; i < m; ++i) {
+        int64_t *g = (int64_t *)malloc(sizeof(int64_t) * (s + 2));
+        for (int j = 0; j < n; ++j) {
+            double v = 0.0;
+            for (int sl = 0; sl < slices; ++sl) {
+                const int k0 = sl * kbs * 32, k1 = (sl + 1) * kbs * 32 < k ? (sl + 1) * kbs * 32 : k;
+                for (int d = 0; d < s + 2; ++d) g[d] = 0;
+                for (int t = 1; t <= s; ++t)
+                    for (int u = 1; t + u <= s + 1; ++u) {
+                        const int8_t *pa = da + ((size_t)(t - 1) * m + i) * kp;
+                        const int8_t *pb = db + ((size_t)(u - 1) * n + j) * kp;
+                        int64_t acc = 0;
+                        for (int kk = k0; kk < k1; ++kk) acc += (int64_t)pa[kk] * pb[kk];
+                        g[t + u] += acc;
+                    }
+                double h = (double)(int32_t)g[s + 1];
+                for (int d = s; d >= 2; --d) h = fma(h, 0.0078125, (double)(int32_t)g[d]);
+                const double r = scale2(h, ea[i] + eb[j] - 12);
+                v = sl == 0 ? r : v + r;
+            }
+            C[(size_t)i * ldc + j] = beta_one ? C[(size_t)i * ldc + j] + v : v;
+        }
+        free(g);
+    }
+    free(da);
+    free(db);
+    free(ea);
+    free(eb);
+    return 0;
+}
+
 /* Number of threads OpenMP will use by default (the host cores this process may run on). */
 ORACLE_API int oracle_max_threads(void) { return omp_get_max_threads(); }

@@ -48,6 +48,8 @@ def lib():
         L.oracle_ozaki_kmax.restype = i
         L.oracle_ozaki_gemm.argtypes = [_dp, _dp, _dp, i, i, i, i, i, i, i, i, i]
         L.oracle_ozaki_gemm.restype = i
+        L.oracle_ozaki_gemm_splitk.argtypes = [_dp, _dp, _dp, i, i, i, i, i, i, i, i, i, i]
+        L.oracle_ozaki_gemm_splitk.restype = i
         L.oracle_max_threads.restype = i
         _lib = L
     return _lib
@@ -177,6 +179,22 @@ def ozaki_gemm(A, B, s: int, C=None, beta_one: bool = False, threads: int = 0) -
     rc = lib().oracle_ozaki_gemm(_p(A), _p(B), _p(C), m, n, k, k, n, n, s, int(beta_one), threads)
     if rc:
         raise ValueError("non-finite input to the Ozaki form")
+    return C
+
+
+def ozaki_gemm_splitk(A, B, s: int, ksplit: int, C=None, beta_one: bool = False, threads: int = 0) -> np.ndarray:
+    """The Ozaki product with the K range cut into ksplit slices, each recombined on its own and
+    the slice results added in order (the GPU's split-K form; k <= ozaki kmax)."""
+    A, B = _f64(A), _f64(B)
+    m, k = A.shape
+    n = B.shape[1]
+    if C is None:
+        C = np.zeros((m, n), np.float64)
+    rc = lib().oracle_ozaki_gemm_splitk(_p(A), _p(B), _p(C), m, n, k, k, n, n, s, ksplit, int(beta_one), threads)
+    if rc == 1:
+        raise ValueError("non-finite input to the Ozaki form")
+    if rc == 2:
+        raise ValueError("k above one int32 accumulation for this split count")
     return C
 
 

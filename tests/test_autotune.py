@@ -33,15 +33,21 @@ def test_candidates_and_features():
     cs = at.candidates()
     assert cs[0].tile == at.TILE_FP64 and cs[0].splits == 0 and cs[0].ksplit == 1
     assert [c.ksplit for c in cs if c.is_fp64] == [1, 2, 4, 8, 16]
-    assert [c.splits for c in cs if not c.is_fp64] == list(range(3, 10))
+    assert [c.splits for c in cs if not c.is_fp64 and c.ksplit == 1] == list(range(3, 10))
+    assert sorted({c.ksplit for c in cs if not c.is_fp64}) == [1, 4, 16]
+    assert len({c.name for c in cs}) == len(cs) == 5 + 3 * 7
     oz5 = next(c for c in cs if c.splits == 5)
     f = at.features(1024, 2048, 4096, 20, oz5)
     assert f[:3] == [10.0, 11.0, 12.0] and f[3:] == [20.0, 1.0, 5.0]
     # split-K candidates only where the K range has the blocks and the slices fit the workspace cap
     small = at.candidates(300, 300, 100)            # 4 K blocks
     assert [c.ksplit for c in small if c.is_fp64] == [1, 2, 4]
+    assert sorted({c.ksplit for c in small if not c.is_fp64}) == [1, 4]
     big = at.candidates(32768, 32768, 32768)
-    assert [c.ksplit for c in big if c.is_fp64] == [1]
+    assert [c.ksplit for c in big if c.is_fp64] == [1] and {c.ksplit for c in big} == {1}
+    # an Ozaki K slice needs K within one int32 accumulation
+    assert at.ozaki_kmax(9) == 58240 and not at.splitk_applies(64, 64, 60000, 4, 9)
+    assert at.splitk_applies(64, 64, 60000, 4, 8)
 
 
 def test_random_shapes_and_memory_bound():

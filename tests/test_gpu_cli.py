@@ -76,3 +76,17 @@ def test_mm2d_random_inputs_error_check():
     r = launch("mm_2d", 4, 512, "MMM", MGXBENCH_INPUT="uniform", MGXBENCH_FORM="fp64", MGXBENCH_CHECK_ROWS=64)
     rec = parse_result(r.stdout)
     assert r.returncode == 0 and rec["valid"] == "1" and float(rec["norm_rel_err"]) < 1e-14
+
+
+@pytest.mark.parametrize("exe,ranks,n,code,env", [("mm_1d", 2, 1024, 2, {}),
+                                                   ("mm_2d", 4, 1024, 1, {"MGXBENCH_SUMMA_BK": 256})])
+def test_inaccurate_result_is_invalid_with_nonzero_exit(exe, ranks, n, code, env):
+    """A result outside its tolerance is reported valid=0 with the reference's failure exit code
+    (1D: 2, 1D-row-block/mmb.cu:1036; 2D: 1, 2D-block-matrix/mmb.cu:439), the contract benchmark.py
+    relies on (benchmark.py:147-156): here the Ozaki form with only 3 slices (normwise error
+    ~1e-6) on wide-range inputs, against the 1e-15 tolerance of that form."""
+    r = launch(exe, ranks, n, "MMM", MGXBENCH_FORM="ozaki", MGXBENCH_SPLITS=3, MGXBENCH_INPUT="wide",
+               MGXBENCH_CHECK_ROWS=64, MGXBENCH_INNER_LOOPS=1, **env)
+    assert r.returncode == code, r.stdout + r.stderr
+    rec = parse_result(r.stdout)
+    assert rec["valid"] == "0" and float(rec["norm_rel_err"]) > 1e-12

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from conftest import rng_matrix
-from gpu_util import bits, dev, host
+from gpu_util import bits, dev, host, vp
 
 pytestmark = pytest.mark.gpu
 
@@ -124,3 +124,50 @@ def test_host_buffer_entry_point_matches_device_path(mgx, oracle, form, panels, 
     mgx.gemm_host(hA, hB, hC2, form=form, splits=8, panels=panels)
     torch.cuda.synchronize()
     assert np.array_equal(bits(hC2.numpy()), bits(hC.numpy()))
+
+
+@pytest.mark.parametrize("m,n,k,s,ks", [(200, 150, 2000, 8, 4), (129, 257, 300, 7, 2), (7, 9, 13, 8, 8),
+                                         (333, 127, 1000, 8, 16), (256, 256, 4096, 9, 64), (64, 66, 64, 3, 3)])
+def test_splitk_bit_identical_to_oracle(mgx, oracle, m, n, k, s, ks):
+    """Ozaki split-K: per-slice recombination, slices added in order -- integer work and the same
+    FP64 operations as the oracle's restatement, so bit-identical; normwise error as unsplit."""
+    import torch
+    rng = np.random.default_rng(m + n + k + s + ks)
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    dA, dB = dev(A), dev(B)
+    dC = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki(dA, dB, dC, splits=s, ksplit=ks)
+    ref = oracle.ozaki_gemm_splitk(A, B, s, ks)
+    assert np.array_equal(bits(host(dC)), bits(ref))
+    # deterministic, and beta_one adds into C
+    C0 = rng_matrix(rng, (m, n))
+    dC2 = dev(C0)
+    mgx.gemm_ozaki(dA, dB, dC2, splits=s, ksplit=ks, beta_one=True)
+    assert np.array_equal(bits(host(dC2)), bits(oracle.ozaki_gemm_splitk(A, B, s, ks, C=C0.copy(), beta_one=True)))
+    assert mgx.device_status() == 0
+
+
+def test_splitk_limits(mgx, oracle):
+    import torch
+    rng = np.random.default_rng(3)
+    m, n, k = 100, 90, 700
+    A, B = rng_matrix(rng, (m, k)), rng_matrix(rng, (k, n))
+    dA, dB = dev(A), dev(B)
+    dC = torch.empty((m, n), dtype=torch.float64, device="cuda")
+    # one slice is the plain Ozaki product
+    mgx.gemm_ozaki(dA, dB, dC, splits=8, ksplit=1)
+    assert np.array_equal(bits(host(dC)), bits(oracle.ozaki_gemm(A, B, 8)))
+    need = mgx.ozaki_splitk_workspace_size(m, n, k, 8, 4)
+    assert need >= mgx.ozaki_workspace_size(m, n, k, 8) + 4 * m * n * 8
+    small = torch.empty(need - 512, dtype=torch.uint8, device="cuda")
+    L = mgx.lib()
+    rc = L.mgx_gemm_ozaki_splitk(vp(dA), vp(dB), vp(dC), m, n, k, k, n, n, 0, 8, 4, vp(small), small.numel(), None)
+    assert rc == -5  # MGX_E_WORKSPACE
+    kk = mgx.ozaki_kmax(12) + 32
+    assert mgx.ozaki_splitk_workspace_size(8, 8, kk, 12, 4) == 0
+    big = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
+    Ak = torch.zeros((8, kk), dtype=torch.float64, device="cuda")
+    Bk = torch.zeros((kk, 8), dtype=torch.float64, device="cuda")
+    Ck = torch.empty((8, 8), dtype=torch.float64, device="cuda")
+    rc = L.mgx_gemm_ozaki_splitk(vp(Ak), vp(Bk), vp(Ck), 8, 8, kk, kk, 8, 8, 0, 12, 4, vp(big), big.numel(), None)
+    assert rc == -6  # MGX_E_UNSUPPORTED: k above one int32 accumulation

@@ -151,3 +151,20 @@ def test_ozaki_kmax_bounds_int32(oracle):
     for s in range(2, 13):
         km = oracle.ozaki_kmax(s)
         assert s * 64 * 64 * km < 2 ** 31 <= s * 64 * 64 * (km + 1)
+
+
+def test_ozaki_splitk_restatement(oracle):
+    """The split-K restatement: one slice is the plain form bit for bit; more slices change only
+    the final additions (same exponents and digits), so the error stays at the unsplit level."""
+    rng = np.random.default_rng(21)
+    A = rng.uniform(-1, 1, (40, 700)) * np.exp2(rng.integers(-20, 21, (40, 700)))
+    B = rng.uniform(-1, 1, (700, 33)) * np.exp2(rng.integers(-20, 21, (700, 33)))
+    one = oracle.ozaki_gemm_splitk(A, B, 8, 1)
+    assert np.array_equal(one.view(np.uint64), oracle.ozaki_gemm(A, B, 8).view(np.uint64))
+    ref = oracle.gemm_dd(A, B)
+    e1 = oracle.error_metrics(one, ref)["normwise"]
+    for ks in (2, 5, 22, 100):
+        e = oracle.error_metrics(oracle.ozaki_gemm_splitk(A, B, 8, ks), ref)["normwise"]
+        assert e <= 2 * e1 + 1e-16
+    with pytest.raises(ValueError):
+        oracle.ozaki_gemm_splitk(np.zeros((2, 70000)), np.zeros((70000, 2)), 8, 2)
