@@ -158,8 +158,8 @@ MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ldc, int beta
 MGX_API int mgx_ozaki_kmax(int splits);
 
 /* C = A B from HOST buffers (hA m x k, hB k x n, hC m x n, row-major, leading dimensions in
- * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  A is cut into `panels` row panels and B
- * into `panels` column panels (multiples of 128); the panels are copied in the order A_0, B_0,
+ * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  A is cut into `panels` (1..64) row panels
+ * and B into `panels` column panels (multiples of 128); the panels are copied in the order A_0, B_0,
  * A_1, B_1, ... and every block (i, j) is computed as soon as A_i and B_j are on the device, then
  * copied back while the rest computes, so PCIe copies in both directions overlap the product.
  * The result is bit-identical to the device-buffer entry points'.  Device memory (A, B, C and

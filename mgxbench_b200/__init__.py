@@ -208,6 +208,8 @@ class OzakiWorkspace:
         return self.buf
 
 
+# Shared by calls that pass no workspace.  Calls that may run concurrently on different streams
+# must each pass their own OzakiWorkspace (a shared one would be overwritten in flight).
 _default_ws = OzakiWorkspace()
 
 

@@ -1053,6 +1053,7 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
     if (m == 0 || n == 0) return MGX_SUCCESS;
     cudaStream_t s0 = (cudaStream_t)stream;
     if (panels < 1) panels = 1;
+    if (panels > 64) panels = 64;  // 64 x 64 blocks at most: one event per block
     const bool ozaki = form == MGX_FORM_OZAKI && k > 0;
     if (ozaki && k > ozaki_kmax(splits)) {
         mgx_set_last_message("mgx_gemm_host: k = %d is above one int32 accumulation (%d) for %d splits", k,
