@@ -278,6 +278,12 @@ MGX_API int mgx_mlp_adam_step(float *params, const float *grads, float *m, float
  * cache.  Later calls allocate again.  No counterpart in MGXBench. */
 MGX_API int mgx_scratch_trim(void);
 
+/* Exercises the timeout path of the library's bounded device-side waits: a kernel waits on a
+ * barrier that nothing completes, gives up after `limit_us` microseconds (1 .. 2e6), records
+ * the timeout in the device status word (read it with mgx_device_status) and returns; the
+ * context stays usable.  Synchronises the device.  No counterpart in MGXBench. */
+MGX_API int mgx_wait_probe(int limit_us);
+
 /* Reads and clears the current device's status word written by bounded device-side waits
  * (0 = none).  Synchronises the device. */
 MGX_API int mgx_device_status(int *code_out);

@@ -82,6 +82,7 @@ EXPORTS = [
     ("mgx_fill_matrix", _i, [_vp, _i, _i, _i, _i, _d, _i, _u64, _vp]),
     ("mgx_device_status", _i, [ctypes.POINTER(_i)]),
     ("mgx_scratch_trim", _i, []),
+    ("mgx_wait_probe", _i, [_i]),
     ("mgx_last_error_message", ctypes.c_char_p, []),
     ("mgx_status_string", ctypes.c_char_p, [_i]),
     ("mgx_peak_fp64", _i, [_i, _i, ctypes.POINTER(_d)]),

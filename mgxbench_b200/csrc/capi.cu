@@ -218,6 +218,38 @@ MGX_API const char *mgx_status_string(int status)
     }
 }
 
+namespace mgx {
+// One thread waits on an mbarrier that nothing ever completes: its bounded wait runs out after
+// limit_ns and records the timeout in the status word, and the kernel returns normally.
+__global__ void wait_probe_kernel(int *status, unsigned long long limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_wait_for(&bar, 0, status, kDevTimeoutFull, limit_ns);
+}
+}  // namespace mgx
+
+MGX_API int mgx_wait_probe(int limit_us)
+{
+    if (limit_us < 1 || limit_us > 2000000) {
+        mgx_set_last_message("mgx_wait_probe: limit %d us outside 1 .. 2000000", limit_us);
+        return MGX_E_INVALID;
+    }
+    int *status = mgx_device_status_ptr();
+    if (!status) {
+        mgx_set_last_message("no device status word (no CUDA device?)");
+        return MGX_E_CUDA;
+    }
+    mgx::wait_probe_kernel<<<1, 32>>>(status, (unsigned long long)limit_us * 1000ull);
+    MGX_HOST_CHECK(cudaGetLastError());
+    MGX_HOST_CHECK(cudaDeviceSynchronize());
+    return MGX_SUCCESS;
+}
+
 MGX_API int mgx_device_status(int *code_out)
 {
     int *p = mgx_device_status_ptr();

@@ -105,9 +105,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`.  Returns false (and records `code`) when the wait
-// ran out; the caller then abandons its loop.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status, int code)
+// Wait for phase `parity` of `bar` for at most `limit_ns`.  Returns false (and records `code`)
+// when the wait ran out; the caller then abandons its loop.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, uint32_t parity, int *status, int code,
+                                              unsigned long long limit_ns)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
@@ -115,12 +116,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((++spins & 255u) == 0u) {
-            if (global_ns() - t0 > kWaitLimitNs) {
+            if (global_ns() - t0 > limit_ns) {
                 record_status(status, code);
                 return false;
             }
         }
     }
+}
+
+// Bounded wait with the library's limit (kWaitLimitNs).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status, int code)
+{
+    return mbar_wait_for(bar, parity, status, code, kWaitLimitNs);
 }
 
 // Bounded wait for waits expected to be long (a warp idling through a whole phase of another
