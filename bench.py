@@ -253,8 +253,12 @@ def run_ours(args):
         e1.synchronize()
         nat_ms = e0.elapsed_time(e1) / reps
         nerr = mgx.error_vs_dd(A, B, C2, row_start=(n - CHECK_ROWS) // 2, row_count=CHECK_ROWS)
-        native = {"tflops": flop / (nat_ms * 1e-3) / 1e12, "ms_per_step": nat_ms, "normwise_err": nerr["normwise"],
+        # the FP64 tensor-core peak, measured on this GPU by the library's DMMA loops (m16n8k8 / k16)
+        fp64_peak = max(mgx.peak_fp64(3, 20000), mgx.peak_fp64(4, 20000))
+        nat_tf = flop / (nat_ms * 1e-3) / 1e12
+        native = {"tflops": nat_tf, "ms_per_step": nat_ms, "normwise_err": nerr["normwise"],
                   "max_rel_err": nerr["max_rel"], "meets_1e-15": nerr["normwise"] <= ERROR_GATE,
+                  "fp64_peak_tflops": fp64_peak, "frac_of_fp64_peak": nat_tf / fp64_peak,
                   "kernel": "dgemm_kernel (DMMA m16n8k8, TMA, warp-specialised)"}
         del C2
 
@@ -294,19 +298,25 @@ def run_ours(args):
 
     # roofline of the dominant kernel (ozaki_gemm): int8 tensor ops per launch / launch time.
     # The INT8 peak is not in MEASURED_PEAKS.json; it is measured here, on this GPU, by the
-    # library's tcgen05 kind::i8 loop (M=128 N=128 K=32, operands resident in shared memory).
+    # library's tcgen05 kind::i8 loop (M=128 N=128 K=32, operands resident in shared memory):
+    # a short burst before the timed region, and a sustained figure -- one launch of about
+    # 2.5 s, long enough for the 1 kW power cap to set the clock -- after it.  ozaki_gemm runs
+    # ~100 ms launches back to back inside a long step, so the sustained figure is its ceiling.
+    int8_sustained = mgx.peak_int8(1, 60_000_000)
     bf16_burst, bf16_sust, hbm, peak_kind = peaks()
     pairs = splits * (splits + 1) // 2
     kp = (n + 31) // 32 * 32
     int8_ops = 2.0 * n * n * kp * pairs
     gemm_avg_ms = sum(gemm_ms) / len(gemm_ms)
     achieved = int8_ops / (gemm_avg_ms * 1e-3) / 1e12
-    peak = int8_peak
+    peak = int8_sustained
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": OZAKI_GEMM_TRAFFIC_BYTES, "kernel": "ozaki_gemm",
                 "peak_note": (f"INT8 dense peak measured on this GPU by mgx_peak_int8 (tcgen05.mma kind::i8 "
-                              f"128x128x32 loop, {int8_peak:.0f} TOP/s); 2 x the {peak_kind} bf16 cuBLAS burst "
-                              f"would be {2 * bf16_burst:.0f}"),
+                              f"128x128x32 loop): sustained over one ~2.5 s launch {int8_sustained:.0f} TOP/s (used), "
+                              f"burst {int8_peak:.0f} TOP/s; 2 x the {peak_kind} bf16 cuBLAS burst would be "
+                              f"{2 * bf16_burst:.0f}"),
+                "peak_burst": int8_peak, "frac_of_burst": achieved / int8_peak,
                 "frac_of_2x_bf16_burst": achieved / (2.0 * bf16_burst),
                 "ops_per_launch": int8_ops, "launch_ms": gemm_avg_ms,
                 "split_ms": ms_per_step - gemm_avg_ms}

@@ -43,7 +43,6 @@ constexpr int SLICE_TILE_BYTES = TILE * KBLK;  // 4 KiB
 constexpr int MAX_SPLITS = 12;
 constexpr int MAX_SETS = 3;            // ceil(12 / 4): up to four weight groups (4 x 128 TMEM columns) per set
 constexpr int EPI_WARPS = 8;
-constexpr int PREFETCH_STAGES = 4;     // how far ahead the producer warms L2 with slabs
 constexpr int THREADS = (2 + EPI_WARPS) * 32;
 constexpr int NONFINITE_EXP = 0x7fffffff;
 
@@ -480,12 +479,6 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
                             // slices 1..nsl of K block kb0+j are contiguous: one bulk copy per operand
                             bulk_load(sa + j * bytes, ga + (size_t)(kb0 + j) * slab, bytes, &full[stage]);
                             bulk_load(sb + j * bytes, gb + (size_t)(kb0 + j) * slab, bytes, &full[stage]);
-                        }
-                        // warm L2 with the slabs this CTA will copy PREFETCH_STAGES stages from now
-                        const int kbp = kb0 + PREFETCH_STAGES * kpack;
-                        for (int j = 0; j < kpack && kbp + j < kb_end; ++j) {
-                            bulk_prefetch_l2(ga + (size_t)(kbp + j) * slab, bytes);
-                            bulk_prefetch_l2(gb + (size_t)(kbp + j) * slab, bytes);
                         }
                         if (++stage == p.stages) {
                             stage = 0;
