@@ -82,9 +82,13 @@ int main(int argc, char *argv[])
     const bool chunked = (libB == 'S' || libB == 'Y' || libB == 'X');
     int splits = mm::env_int("MGXBENCH_SPLITS", 8);
     int ksplit = mm::env_int("MGXBENCH_KSPLIT", 1);
+    const bool batched = mm::env_int("MGXBENCH_BATCH", 1) != 0;
+    const int launches = batched ? 1 : nRanks;
+    const int rows_per_launch = batched ? m : mi;
     const bool autotuned = form == mm::kAuto;
-    // the choice is made for the product each emulated rank runs (its K chunk when chunked)
-    mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, mi, n, chunked ? std::min(pipeline_k_chunk, k) : k,
+    // the choice is made for the product one launch runs (its K chunk when chunked)
+    mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, rows_per_launch, n,
+                          chunked ? std::min(pipeline_k_chunk, k) : k,
                           input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, EXIT_FAILURE, chunked);
     if (chunked) ksplit = 1;
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
@@ -92,7 +96,7 @@ int main(int argc, char *argv[])
            form_name.c_str(), form == mm::kOzaki ? (std::string(" splits=") + std::to_string(splits)).c_str() : "",
            input_name.c_str(), chunked ? "K-chunked" : "single");
     if (chunked) printf(" K-chunk=%d", pipeline_k_chunk);
-    printf("\n");
+    printf(" launches=%s\n", batched ? "one for all ranks" : "one per rank");
 
     const size_t elems = (size_t)m * k;
     double *d_A = nullptr, *d_B = nullptr, *d_C = nullptr;
@@ -115,11 +119,15 @@ int main(int argc, char *argv[])
     mm::cuda_or_die(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate", EXIT_FAILURE);
     mm::Workspace ws;
 
-    // One iteration of the hot loop's compute phase for every emulated rank.
+    // One iteration of the hot loop's compute phase for every emulated rank.  The ranks' row
+    // blocks are contiguous in A and C, and every element of C comes out of the same arithmetic
+    // whatever the launch it belongs to, so by default all ranks' blocks run as one launch
+    // (no tail wave per rank); MGXBENCH_BATCH=0 launches rank by rank.
     auto iteration = [&]() -> int {
-        for (int r = 0; r < nRanks; ++r) {
-            const double *A_r = d_A + (size_t)r * mi * k;
-            double *C_r = d_C + (size_t)r * mi * n;
+        for (int r = 0; r < launches; ++r) {
+            const double *A_r = d_A + (size_t)r * rows_per_launch * k;
+            double *C_r = d_C + (size_t)r * rows_per_launch * n;
+            const int mi = rows_per_launch;
             if (chunked) {
                 cudaError_t e = cudaMemsetAsync(C_r, 0, (size_t)mi * n * sizeof(double), stream);
                 if (e != cudaSuccess) return MGX_E_CUDA;

@@ -90,3 +90,18 @@ def test_inaccurate_result_is_invalid_with_nonzero_exit(exe, ranks, n, code, env
     assert r.returncode == code, r.stdout + r.stderr
     rec = parse_result(r.stdout)
     assert rec["valid"] == "0" and float(rec["norm_rel_err"]) > 1e-12
+
+
+@pytest.mark.parametrize("lib,form", [("MMM", "fp64"), ("SSS", "fp64"), ("MMM", "ozaki"), ("XXX", "ozaki")])
+def test_mm1d_batched_ranks_give_the_same_result(lib, form):
+    """All ranks' row blocks in one launch (default) or rank by rank: every element comes out of
+    the same arithmetic, so the accuracy record is identical to the last digit printed."""
+    recs = []
+    for batch in (1, 0):
+        r = launch("mm_1d", 4, 1024, lib, MGXBENCH_BATCH=batch, MGXBENCH_FORM=form, MGXBENCH_INPUT="wide",
+                   MGXBENCH_CHECK_ROWS=1024, MGXBENCH_INNER_LOOPS=1, MM_PIPELINE_K_CHUNK=256)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert ("one for all ranks" if batch else "one per rank") in r.stdout
+        recs.append(parse_result(r.stdout))
+    assert recs[0]["valid"] == recs[1]["valid"] == "1"
+    assert recs[0]["norm_rel_err"] == recs[1]["norm_rel_err"] and recs[0]["max_rel_err"] == recs[1]["max_rel_err"]
