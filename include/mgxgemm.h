@@ -157,6 +157,32 @@ MGX_API int mgx_ozaki_multiply(double *C, int m, int n, int k, int ldc, int beta
  * into chunks of this size and adds them in order). */
 MGX_API int mgx_ozaki_kmax(int splits);
 
+/* ------------------------------------------------------------------------------------------
+ * CRT form (Ozaki scheme II): one INT8 tensor-core product per modulus
+ * ------------------------------------------------------------------------------------------ */
+
+/* Bytes of device workspace mgx_gemm_ozaki_crt needs for this shape and modulus count. */
+MGX_API size_t mgx_crt_workspace_size(int m, int n, int k, int moduli);
+
+/* C = A B or C += A B computed as `moduli` (8..16) INT8 products of residues: each row of A and
+ * column of B is scaled by a power of two to integers whose norms leave every exact integer
+ * product below a quarter of the moduli's product, the integers are reduced modulo pairwise-coprime
+ * p_l <= 256, each residue product runs on the tensor cores (exact int32) and is reduced mod p_l,
+ * and C is rebuilt in FP64 by the Chinese remainder theorem.  15 moduli reach FP64 accuracy at
+ * K = 16384 with 15 products, where the slice form needs 36 for 8 slices.  Rows or columns
+ * holding NaN or infinity give NaN results and set the device status (mgx_device_status).
+ * No counterpart in MGXBench. */
+MGX_API int mgx_gemm_ozaki_crt(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                               int ldb, int ldc, int beta_one, int moduli, void *workspace,
+                               size_t workspace_bytes, void *stream);
+
+/* Smallest modulus count whose a-priori normwise error bound meets `target` for reduction
+ * length k (8..16). */
+MGX_API int mgx_crt_choose_moduli(int k, double target);
+
+/* Largest K of one int32 residue accumulation (longer K is processed in chunks of this size). */
+MGX_API int mgx_crt_kmax(void);
+
 /* C = A B from HOST buffers (hA m x k, hB k x n, hC m x n, row-major, leading dimensions in
  * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  A is cut into `panels` (1..64) row panels
  * and B into `panels` column panels (multiples of 128); the panels are copied in the order A_0, B_0,

@@ -71,6 +71,10 @@ EXPORTS = [
     ("mgx_ozaki_split", _i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_multiply", _i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_kmax", _i, [_i]),
+    ("mgx_crt_workspace_size", _sz, [_i, _i, _i, _i]),
+    ("mgx_gemm_ozaki_crt", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_crt_choose_moduli", _i, [_i, _d]),
+    ("mgx_crt_kmax", _i, []),
     ("mgx_gemm_ozaki_noalloc", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
     ("mgx_gemm_host", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
     ("mgx_summa_tiles", _i, [ctypes.POINTER(SummaDesc), ctypes.POINTER(_i), _i]),
@@ -235,6 +239,31 @@ def gemm_ozaki(A, B, C, splits: int = 8, beta_one: bool = False, workspace=None,
     return _check(lib().mgx_gemm_ozaki(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
                                        int(beta_one), splits, _ptr(ws), ws.numel(), _stream(stream)),
                   "mgx_gemm_ozaki")
+
+
+def crt_workspace_size(m, n, k, moduli) -> int:
+    return int(lib().mgx_crt_workspace_size(m, n, k, moduli))
+
+
+def gemm_ozaki_crt(A, B, C, moduli: int = 15, beta_one: bool = False, workspace=None, stream=None):
+    """C (+)= A B by the CRT form (Ozaki scheme II): one INT8 tensor-core product per modulus,
+    FP64 result rebuilt by the Chinese remainder theorem (mgx_gemm_ozaki_crt)."""
+    _check_f64(A, B, C)
+    m, k = A.shape
+    n = B.shape[1]
+    need = crt_workspace_size(m, n, k, moduli)
+    ws = (workspace or _default_ws).get(need)
+    return _check(lib().mgx_gemm_ozaki_crt(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
+                                           int(beta_one), moduli, _ptr(ws), ws.numel(), _stream(stream)),
+                  "mgx_gemm_ozaki_crt")
+
+
+def crt_choose_moduli(k: int, target: float = 1e-15) -> int:
+    return int(lib().mgx_crt_choose_moduli(k, target))
+
+
+def crt_kmax() -> int:
+    return int(lib().mgx_crt_kmax())
 
 
 def ozaki_split(A, B, splits: int, workspace, stream=None):

@@ -685,5 +685,222 @@ ORACLE_API int oracle_ozaki_gemm_splitk(const double *A, const double *B, double
     return 0;
 }
 
+/* ------------------------------------------------------------------------------------------
+ * 6. Ozaki scheme II restatement (the CRT form; Ozaki, Uchino & Imamura 2025, "Ozaki Scheme
+ *    II: a GEMM-oriented emulation of floating-point matrix multiplication using an integer
+ *    modular technique").  Bit-exact model of the GPU form:
+ *
+ *    moduli  p_1..p_q: the first q of 256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223,
+ *            217, 211, 199, 197, 193 (pairwise coprime), P = p_1 ... p_q, L = bit length of P.
+ *    scale   row i of A: e = frexp exponent of max|a_ik|; c_k = max(1, ceil(|a_ik| 2^(22-e)))
+ *            for a_ik != 0; S = sum c_k^2 (uint64, so independent of the order);
+ *            u = ceil(log2(S) / 2) = (bitlen(S - 1) + 1) / 2; sigma_i = alpha - e + 22 - u, so
+ *            2^sigma_i ||a_i||_2 <= 2^alpha.  Columns of B likewise with beta.
+ *            alpha = (L - 3) / 2, beta = L - 3 - alpha: by Cauchy-Schwarz every exact integer
+ *            product C'_ij = sum_k A'_ik B'_kj of the scaled, rounded operands
+ *            A' = rint(2^sigma A), B' = rint(B 2^tau) has |C'_ij| < P / 4.
+ *    residues  A'_ik mod p_l as int8 in [-(p-1)/2, (p-1)/2] ([-128, 127] for 256); B' likewise.
+ *    products  R_l = (sum_k rA_l rB_l) mod p_l in [0, p_l): exact in int32 for k <= 130816.
+ *    CRT     w_l = (P / p_l) ((P / p_l)^-1 mod p_l) < P, cut into three 40-bit chunks
+ *            w_l = w1 2^E1 + w2 2^E2 + w3 2^E3 (E_t = L - 40 t); P likewise.
+ *            s_t = sum_l w_t,l R_l (exact in FP64: < 16 2^40 2^8 = 2^52),
+ *            Q = rint(fma(s2, 2^-40, s1) / P~) is the nearest integer to sum w R / P,
+ *            d_t = fma(-Q, P_t, s_t) (exact), c = fma(fma(d1, 2^40, d2), 2^40, d3),
+ *            C_ij = c 2^(E3 - sigma_i - tau_j) = C'_ij 2^(-sigma_i - tau_j) to FP64 rounding.
+ *    K beyond 130816 is processed in chunks, each scaled on its own and added into C in order.
+ * ------------------------------------------------------------------------------------------ */
+#define CRT_MAX_MODULI 16
+#define CRT_KMAX 130816
+static const int crt_moduli[CRT_MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                               229, 227, 223, 217, 211, 199, 197, 193};
+
+typedef struct {
+    int q, L, alpha, beta, E3;
+    double w[CRT_MAX_MODULI][3];
+    double pc[3];
+    double inv_phat;
+} crt_consts_t;
+
+static void crt_chunks(unsigned __int128 v, int L, double out[3])
+{
+    for (int t = 0; t < 3; ++t) {
+        const int e = L - 40 * (t + 1);
+        unsigned __int128 c;
+        if (e >= 0) {
+            c = v >> e;
+            v -= c << e;
+        } else {
+            c = v << (-e);
+            v = 0;
+        }
+        out[t] = (double)(uint64_t)c; /* < 2^40 */
+    }
+}
+
+static int crt_consts(int q, crt_consts_t *K)
+{
+    if (q < 8 || q > CRT_MAX_MODULI) return 1;
+    unsigned __int128 P = 1;
+    for (int l = 0; l < q; ++l) P *= (unsigned)crt_moduli[l];
+    int L = 0;
+    for (unsigned __int128 t = P; t; t >>= 1) ++L;
+    K->q = q;
+    K->L = L;
+    K->alpha = (L - 3) / 2;
+    K->beta = L - 3 - K->alpha;
+    K->E3 = L - 120;
+    for (int l = 0; l < q; ++l) {
+        const unsigned p = (unsigned)crt_moduli[l];
+        const unsigned __int128 M = P / p;
+        const unsigned mm = (unsigned)(M % p);
+        unsigned inv = 1;
+        while ((mm * inv) % p != 1) ++inv;
+        crt_chunks(M * inv, L, K->w[l]);
+    }
+    crt_chunks(P, L, K->pc);
+    K->inv_phat = 1.0 / fma(K->pc[1], 0x1p-40, K->pc[0]);
+    return 0;
+}
+
+static int bitlen64(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
+
+/* sigma of one row (stride 1) or column (stride ldb) of k values; *nonfinite set on Inf/NaN. */
+static int crt_sigma(const double *v, size_t stride, int k, int target, int *nonfinite)
+{
+    uint64_t mx = 0;
+    for (int kk = 0; kk < k; ++kk) {
+        uint64_t b;
+        memcpy(&b, &v[(size_t)kk * stride], 8);
+        b &= 0x7fffffffffffffffull;
+        if (b >= 0x7ff0000000000000ull) *nonfinite = 1;
+        if (b > mx) mx = b;
+    }
+    if (mx == 0 || mx >= 0x7ff0000000000000ull) return 0;
+    const int e = frexp_exp_bits(mx);
+    uint64_t S = 0;
+    for (int kk = 0; kk < k; ++kk) {
+        const double x = fabs(v[(size_t)kk * stride]);
+        if (x == 0.0) continue;
+        double c = ceil(scale2(x, 22 - e));
+        if (c < 1.0) c = 1.0;
+        const uint64_t ci = (uint64_t)c;
+        S += ci * ci;
+    }
+    const int u = (bitlen64(S - 1) + 1) / 2;
+    return target - e + 22 - u;
+}
+
+/* Symmetric residue of the integer x (|x| < 2^63) modulo p. */
+static int8_t crt_residue(int64_t x, int p)
+{
+    if (p == 256) return (int8_t)(uint8_t)(x & 255);
+    int64_t r = x % p;
+    if (r < 0) r += p;
+    if (r > p / 2) r -= p;
+    return (int8_t)r;
+}
+
+/* Scale exponents (sigma for the rows of A, tau for the columns of B) of one K range.
+ * Returns 1 on non-finite input. */
+ORACLE_API int oracle_crt_scales(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int q,
+                                 int32_t *sigma, int32_t *tau)
+{
+    crt_consts_t K;
+    if (crt_consts(q, &K)) return 2;
+    int nonfinite = 0;
+    for (int i = 0; i < m; ++i) sigma[i] = crt_sigma(A + (size_t)i * lda, 1, k, K.alpha, &nonfinite);
+    for (int j = 0; j < n; ++j) tau[j] = crt_sigma(B + j, (size_t)ldb, k, K.beta, &nonfinite);
+    return nonfinite;
+}
+
+/* Residues of A as [l][i][kp] and of B^T as [l][j][kp] (int8, padding zero). */
+ORACLE_API void oracle_crt_residues(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int q,
+                                    int kp, const int32_t *sigma, const int32_t *tau, int8_t *ra, int8_t *rb)
+{
+    memset(ra, 0, (size_t)q * m * kp);
+    memset(rb, 0, (size_t)q * n * kp);
+    for (int i = 0; i < m; ++i)
+        for (int kk = 0; kk < k; ++kk) {
+            const double a = A[(size_t)i * lda + kk];
+            if (!isfinite(a)) continue;
+            const int64_t x = (int64_t)nearbyint(scale2(a, sigma[i]));
+            for (int l = 0; l < q; ++l) ra[((size_t)l * m + i) * kp + kk] = crt_residue(x, crt_moduli[l]);
+        }
+    for (int j = 0; j < n; ++j)
+        for (int kk = 0; kk < k; ++kk) {
+            const double b = B[(size_t)kk * ldb + j];
+            if (!isfinite(b)) continue;
+            const int64_t x = (int64_t)nearbyint(scale2(b, tau[j]));
+            for (int l = 0; l < q; ++l) rb[((size_t)l * n + j) * kp + kk] = crt_residue(x, crt_moduli[l]);
+        }
+}
+
+/* The CRT recombination of one output from its residues R[0..q) (each in [0, p_l)). */
+static double crt_combine(const crt_consts_t *K, const int32_t *R, int scale)
+{
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int l = 0; l < K->q; ++l) {
+        const double r = (double)R[l];
+        s1 = fma(K->w[l][0], r, s1);
+        s2 = fma(K->w[l][1], r, s2);
+        s3 = fma(K->w[l][2], r, s3);
+    }
+    const double Q = nearbyint(fma(s2, 0x1p-40, s1) * K->inv_phat);
+    const double d1 = fma(-Q, K->pc[0], s1);
+    const double d2 = fma(-Q, K->pc[1], s2);
+    const double d3 = fma(-Q, K->pc[2], s3);
+    const double c = fma(fma(d1, 0x1p40, d2), 0x1p40, d3);
+    return scale2(c, K->E3 + scale);
+}
+
+ORACLE_API int oracle_crt_kmax(void) { return CRT_KMAX; }
+
+/* C = (beta_one ? C + v : v), v = A B by the CRT form with q moduli (8..16).  Returns 1 on
+ * non-finite input (C untouched), 2 on an unsupported q. */
+ORACLE_API int oracle_crt_gemm(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                               int ldc, int q, int beta_one, int nthreads)
+{
+    nthreads = pick_threads(nthreads);
+    crt_consts_t K;
+    if (crt_consts(q, &K)) return 2;
+    int32_t *sg = (int32_t *)malloc(sizeof(int32_t) * (m > 0 ? m : 1));
+    int32_t *tu = (int32_t *)malloc(sizeof(int32_t) * (n > 0 ? n : 1));
+    for (int k0 = 0; k0 < k || k0 == 0; k0 += CRT_KMAX) {
+        const int kc = (k - k0 < CRT_KMAX) ? k - k0 : CRT_KMAX;
+        if (oracle_crt_scales(A + k0, B + (size_t)k0 * ldb, m, n, kc, lda, ldb, q, sg, tu)) {
+            free(sg);
+            free(tu);
+            return 1;
+        }
+        const int kp = (kc + 15) & ~15;
+        int8_t *ra = (int8_t *)malloc((size_t)q * m * kp + 1);
+        int8_t *rb = (int8_t *)malloc((size_t)q * n * kp + 1);
+        oracle_crt_residues(A + k0, B + (size_t)k0 * ldb, m, n, kc, lda, ldb, q, kp, sg, tu, ra, rb);
+        const int add = (k0 > 0) || beta_one;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+        for (int i = 0; i < m; ++i) {
+            int32_t R[CRT_MAX_MODULI];
+            for (int j = 0; j < n; ++j) {
+                for (int l = 0; l < q; ++l) {
+                    const int8_t *pa = ra + ((size_t)l * m + i) * kp;
+                    const int8_t *pb = rb + ((size_t)l * n + j) * kp;
+                    int32_t acc = 0;
+                    for (int kk = 0; kk < kc; ++kk) acc += (int32_t)pa[kk] * (int32_t)pb[kk];
+                    int32_t r = acc % crt_moduli[l];
+                    R[l] = r < 0 ? r + crt_moduli[l] : r;
+                }
+                const double v = crt_combine(&K, R, -sg[i] - tu[j]);
+                C[(size_t)i * ldc + j] = add ? C[(size_t)i * ldc + j] + v : v;
+            }
+        }
+        free(ra);
+        free(rb);
+        if (k == 0) break;
+    }
+    free(sg);
+    free(tu);
+    return 0;
+}
+
 /* Number of threads OpenMP will use by default (the host cores this process may run on). */
 ORACLE_API int oracle_max_threads(void) { return omp_get_max_threads(); }

@@ -50,6 +50,12 @@ def lib():
         L.oracle_ozaki_gemm.restype = i
         L.oracle_ozaki_gemm_splitk.argtypes = [_dp, _dp, _dp, i, i, i, i, i, i, i, i, i, i]
         L.oracle_ozaki_gemm_splitk.restype = i
+        L.oracle_crt_scales.argtypes = [_dp, _dp, i, i, i, i, i, i, _i32p, _i32p]
+        L.oracle_crt_scales.restype = i
+        L.oracle_crt_residues.argtypes = [_dp, _dp, i, i, i, i, i, i, i, _i32p, _i32p, _i8p, _i8p]
+        L.oracle_crt_kmax.restype = i
+        L.oracle_crt_gemm.argtypes = [_dp, _dp, _dp, i, i, i, i, i, i, i, i, i]
+        L.oracle_crt_gemm.restype = i
         L.oracle_max_threads.restype = i
         _lib = L
     return _lib
@@ -195,6 +201,51 @@ def ozaki_gemm_splitk(A, B, s: int, ksplit: int, C=None, beta_one: bool = False,
         raise ValueError("non-finite input to the Ozaki form")
     if rc == 2:
         raise ValueError("k above one int32 accumulation for this split count")
+    return C
+
+
+CRT_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193)
+
+
+def crt_scales(A, B, q: int):
+    """Power-of-two scale exponents of the CRT form: sigma per row of A, tau per column of B."""
+    A, B = _f64(A), _f64(B)
+    m, k = A.shape
+    n = B.shape[1]
+    sg = np.empty(m, np.int32); tu = np.empty(n, np.int32)
+    rc = lib().oracle_crt_scales(_p(A), _p(B), m, n, k, k, n, q, _p(sg, _i32p), _p(tu, _i32p))
+    return sg, tu, rc
+
+
+def crt_residues(A, B, q: int):
+    """Residues of the scaled operands: ra [q, m, kp] and rb [q, n, kp] (B transposed), int8."""
+    A, B = _f64(A), _f64(B)
+    m, k = A.shape
+    n = B.shape[1]
+    sg, tu, rc = crt_scales(A, B, q)
+    kp = (k + 15) & ~15
+    ra = np.empty((q, m, kp), np.int8); rb = np.empty((q, n, kp), np.int8)
+    lib().oracle_crt_residues(_p(A), _p(B), m, n, k, k, n, q, kp, _p(sg, _i32p), _p(tu, _i32p),
+                              _p(ra, _i8p), _p(rb, _i8p))
+    return ra, rb, sg, tu
+
+
+def crt_kmax() -> int:
+    return lib().oracle_crt_kmax()
+
+
+def crt_gemm(A, B, q: int, C=None, beta_one: bool = False, threads: int = 0) -> np.ndarray:
+    """A B by the CRT form (Ozaki scheme II) with q moduli, as the GPU computes it."""
+    A, B = _f64(A), _f64(B)
+    m, k = A.shape
+    n = B.shape[1]
+    if C is None:
+        C = np.zeros((m, n), np.float64)
+    rc = lib().oracle_crt_gemm(_p(A), _p(B), _p(C), m, n, k, k, n, n, q, int(beta_one), threads)
+    if rc == 1:
+        raise ValueError("non-finite input to the CRT form")
+    if rc == 2:
+        raise ValueError(f"{q} moduli: the CRT form takes 8..16")
     return C
 
 

@@ -1,0 +1,111 @@
+"""CRT form (Ozaki scheme II) on the GPU: bit-identical to the oracle's restatement (the scales,
+residues and residue products are integer work; the CRT recombination follows the same FP64
+operations in the same order), and accurate against the double-double product."""
+import numpy as np
+import pytest
+
+from conftest import rng_matrix
+from gpu_util import bits, dev, host
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("m,n,k,q,kind", [
+    (256, 256, 256, 15, "wide"), (1, 1, 1, 8, "uniform"), (77, 200, 333, 14, "wide"),
+    (300, 129, 1000, 15, "uniform"), (513, 257, 96, 16, "wide"), (256, 512, 64, 12, "wide"),
+    (130, 260, 2048, 9, "wide"), (64, 600, 31, 13, "uniform"), (520, 40, 700, 10, "wide"),
+    (257, 255, 4100, 11, "uniform")])
+def test_crt_bit_exact_vs_oracle(mgx, oracle, m, n, k, q, kind):
+    import torch
+    rng = np.random.default_rng(m * 31 + n * 7 + k + q)
+    A, B = rng_matrix(rng, (m, k), kind), rng_matrix(rng, (k, n), kind)
+    dC = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=q)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, q)))
+    assert mgx.device_status() == 0
+
+
+def test_crt_zero_rows_columns_and_extreme_scales(mgx, oracle):
+    """Zero rows/columns (scale 0), rows of subnormals (scale > 1023, two-step) and rows near the
+    top of the range all go through the same integer scaling."""
+    import torch
+    rng = np.random.default_rng(11)
+    A, B = rng_matrix(rng, (300, 500), "wide"), rng_matrix(rng, (500, 270), "wide")
+    A[3] = 0.0
+    B[:, 8] = 0.0
+    A[7] *= 2.0 ** -1060
+    A[9] *= 2.0 ** 900
+    B[:, 11] *= 2.0 ** -700
+    dC = torch.empty((300, 270), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=15)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, 15)))
+    assert mgx.device_status() == 0
+
+
+def test_crt_beta_one(mgx, oracle):
+    rng = np.random.default_rng(3)
+    A, B, C0 = rng_matrix(rng, (200, 300)), rng_matrix(rng, (300, 170)), rng_matrix(rng, (200, 170))
+    dC = dev(C0)
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=14, beta_one=True)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, 14, C=C0.copy(), beta_one=True)))
+
+
+def test_crt_k_beyond_one_int32_accumulation(mgx, oracle):
+    """K longer than one exact int32 residue accumulation runs in chunks added in order."""
+    import torch
+    rng = np.random.default_rng(12)
+    k = mgx.crt_kmax() + 1000
+    assert k - 1000 == oracle.crt_kmax()
+    A, B = rng_matrix(rng, (9, k), "wide"), rng_matrix(rng, (k, 7), "wide")
+    dC = torch.empty((9, 7), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=16)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, 16)))
+
+
+def test_crt_integer_known_answer(mgx):
+    import torch
+    N = 1024
+    A = torch.ones((N, N), dtype=torch.float64, device="cuda")
+    B = torch.full((N, N), 2.0, dtype=torch.float64, device="cuda")
+    C = torch.empty((N, N), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(A, B, C, moduli=8)
+    assert torch.all(C == 2.0 * N)
+
+
+@pytest.mark.parametrize("kind", ["wide", "uniform"])
+def test_crt_accuracy_chosen_moduli(mgx, kind):
+    """The a-priori modulus count meets 1e-15 normwise against the double-double product."""
+    import torch
+    rng = np.random.default_rng(5)
+    k = 4096
+    q = mgx.crt_choose_moduli(k, 1e-15)
+    A, B = rng_matrix(rng, (512, k), kind), rng_matrix(rng, (k, 512), kind)
+    dA, dB = dev(A), dev(B)
+    dC = torch.empty((512, 512), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dA, dB, dC, moduli=q)
+    assert mgx.error_vs_dd(dA, dB, dC)["normwise"] <= 1e-15
+
+
+def test_crt_nonfinite_marks_rows_and_columns(mgx):
+    import torch
+    rng = np.random.default_rng(6)
+    A, B = rng_matrix(rng, (140, 64)), rng_matrix(rng, (64, 150))
+    A[5, 7] = np.inf
+    B[3, 9] = np.nan
+    dC = torch.empty((140, 150), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=15)
+    C = host(dC)
+    assert mgx.device_status() == 4
+    assert np.all(np.isnan(C[5])) and np.all(np.isnan(C[:, 9]))
+    keep = np.ones(140, bool)
+    keep[5] = False
+    assert np.all(np.isfinite(np.delete(C[keep], 9, axis=1)))
+
+
+def test_crt_argument_errors(mgx):
+    import torch
+    A = torch.ones((4, 4), dtype=torch.float64, device="cuda")
+    for q in (7, 17):
+        with pytest.raises(mgx.MgxError):
+            mgx.gemm_ozaki_crt(A, A, A.clone(), moduli=q)
+    assert mgx.crt_workspace_size(4, 4, 4, 7) == 0
