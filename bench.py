@@ -7,10 +7,11 @@ mulmat_kernel.cu:39-92, at the size the headline metric is quoted on).
 
 One step = one C = A B of 16384 x 16384 x 16384 FP64 with wide-exponent inputs
 (u * 2^e, u ~ U[-1,1), e ~ U{-20..20}), A and B resident in HBM (2 GiB each, larger than L2).
-`value` is effective TFLOP/s = 2 N^3 / step time of the Ozaki form (split + tensor-core
-products + FP64 recombination), valid only if its normwise error against a double-double
-product (sampled rows) is <= 1e-15.  `e2e` is the same product through the C ABI with pinned
-host buffers, host-to-device and device-to-host copies inside each step.
+`value` is effective TFLOP/s = 2 N^3 / step time of the Ozaki INT8 form -- by default its CRT
+form (Ozaki scheme II: scales and residues, one tensor-core product per modulus, CRT
+recombination), `--form slices` for the digit-slice form -- valid only if its normwise error
+against a double-double product (sampled rows) is <= 1e-15.  `e2e` is the same product through
+the C ABI with pinned host buffers, host-to-device and device-to-host copies inside each step.
 Under torchrun every rank computes its own independent product (weak scaling, no data-path
 collective); the step time is the max over ranks.
 `--impl reference` times MGXBench's arithmetic on the host cores instead: the oracle's
@@ -37,9 +38,11 @@ N_DEFAULT = 16384
 EXP_RANGE = 20
 ERROR_GATE = 1e-15
 CHECK_ROWS = 256
-# DRAM bytes (read + write) per ozaki_gemm launch at N = 16384, s = 8, from the one-pass ncu
-# capture at full size summarised in profiles/ozaki_gemm_n4096.md (167.53 GB + 2.16 GB).
+# DRAM bytes (read + write) per launch of the dominant kernel at N = 16384, from one-pass ncu
+# captures at full size: ozaki_gemm (s = 8, profiles/ozaki_gemm_n4096.md: 167.53 GB + 2.16 GB)
+# and crt_gemm (q = 15, profiles/crt_gemm_n16384.md).
 OZAKI_GEMM_TRAFFIC_BYTES = 169.69e9
+CRT_GEMM_TRAFFIC_BYTES = None
 
 
 def env_rank():
@@ -190,8 +193,13 @@ def run_ours(args):
     C = torch.empty((n, n), dtype=torch.float64, device="cuda")
     mgx.fill_matrix(A, 2, e_range=EXP_RANGE, seed=1000 + 2 * rank, stream=stream)
     mgx.fill_matrix(B, 2, e_range=EXP_RANGE, seed=1001 + 2 * rank, stream=stream)
+    crt = args.form == "crt"
     splits = args.splits or mgx.ozaki_choose_splits(n, float(EXP_RANGE), ERROR_GATE)
-    ws = torch.empty(mgx.ozaki_workspace_size(n, n, n, splits), dtype=torch.uint8, device="cuda")
+    moduli = args.moduli or mgx.crt_choose_moduli(n, ERROR_GATE)
+    if crt:
+        ws = torch.empty(mgx.crt_workspace_size(n, n, n, moduli), dtype=torch.uint8, device="cuda")
+    else:
+        ws = torch.empty(mgx.ozaki_workspace_size(n, n, n, splits), dtype=torch.uint8, device="cuda")
     stream.synchronize()
 
     def barrier():
@@ -199,10 +207,17 @@ def run_ours(args):
             dist.barrier()
 
     def step():
-        mgx.ozaki_split(A, B, splits, ws, stream=stream)
-        ev_g0.record(stream)
-        mgx.ozaki_multiply(C, n, splits, ws, stream=stream)
-        ev_g1.record(stream)
+        if crt:
+            mgx.crt_split(A, B, moduli, ws, stream=stream)
+            ev_g0.record(stream)
+            mgx.crt_products(n, n, n, moduli, ws, stream=stream)
+            ev_g1.record(stream)
+            mgx.crt_combine(C, n, moduli, ws, stream=stream)
+        else:
+            mgx.ozaki_split(A, B, splits, ws, stream=stream)
+            ev_g0.record(stream)
+            mgx.ozaki_multiply(C, n, splits, ws, stream=stream)
+            ev_g1.record(stream)
 
     ev_g0 = torch.cuda.Event(enable_timing=True)
     ev_g1 = torch.cuda.Event(enable_timing=True)
@@ -225,6 +240,8 @@ def run_ours(args):
         ev_g1.synchronize()
         gemm_ms.append(ev_g0.elapsed_time(ev_g1))
     t_stop.record(stream)
+    # (ev_g1.synchronize() waits for the products only; the next step's split is queued behind
+    # the combine on the same stream, so the steps stay back to back on the GPU.)
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
@@ -262,6 +279,28 @@ def run_ours(args):
                   "kernel": "dgemm_kernel (DMMA m16n8k8, TMA, warp-specialised)"}
         del C2
 
+    # the other Ozaki form on the same inputs (slices when the headline is the CRT form)
+    other = {}
+    if crt and not args.skip_native:
+        C3 = torch.empty_like(C)
+        ws_s = torch.empty(mgx.ozaki_workspace_size(n, n, n, splits), dtype=torch.uint8, device="cuda")
+        mgx.gemm_ozaki(A, B, C3, splits=splits, workspace=_Ws(ws_s), stream=stream)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = max(1, min(args.steps, 3))
+        e0.record(stream)
+        for _ in range(reps):
+            mgx.gemm_ozaki(A, B, C3, splits=splits, workspace=_Ws(ws_s), stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        s_ms = e0.elapsed_time(e1) / reps
+        serr = mgx.error_vs_dd(A, B, C3, row_start=(n - CHECK_ROWS) // 2, row_count=CHECK_ROWS)
+        other = {"form": "ozaki-int8 digit slices", "splits": splits, "tflops": flop / (s_ms * 1e-3) / 1e12,
+                 "ms_per_step": s_ms, "normwise_err": serr["normwise"], "int8_products": splits * (splits + 1) // 2}
+        del C3, ws_s
+        torch.cuda.empty_cache()
+
     # end to end through the C ABI with pinned host buffers: mgx_gemm_host streams row panels of
     # A and column panels of B in, computes each block of C once its two panels are on the device
     # and streams the blocks back while the rest computes
@@ -277,14 +316,17 @@ def run_ours(args):
         del C
         torch.cuda.empty_cache()
         reps = max(1, min(args.steps, 3))
-        mgx.gemm_host(hA, hB, hC, form=mgx.FORM_OZAKI, splits=splits, panels=args.panels, stream=stream)
+        form_id, form_arg = (mgx.FORM_CRT, moduli) if crt else (mgx.FORM_OZAKI, splits)
+        del ws
+        torch.cuda.empty_cache()
+        mgx.gemm_host(hA, hB, hC, form=form_id, splits=form_arg, panels=args.panels, stream=stream)
         stream.synchronize()
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
-            mgx.gemm_host(hA, hB, hC, form=mgx.FORM_OZAKI, splits=splits, panels=args.panels, stream=stream)
+            mgx.gemm_host(hA, hB, hC, form=form_id, splits=form_arg, panels=args.panels, stream=stream)
         e1.record(stream)
         e1.synchronize()
         e2e_ms = ranks_reduce_max(dist, e0.elapsed_time(e1) / reps, "cuda")
@@ -296,7 +338,8 @@ def run_ours(args):
                        f"{args.panels} column panels of B, each block computed once its panels arrive and copied "
                        f"back while the rest computes"}
 
-    # roofline of the dominant kernel (ozaki_gemm): int8 tensor ops per launch / launch time.
+    # roofline of the dominant kernel (crt_gemm, or ozaki_gemm for the slice form): int8 tensor
+    # ops per launch / launch time.
     # The INT8 peak is not in MEASURED_PEAKS.json; it is measured here, on this GPU, by the
     # library's tcgen05 kind::i8 loop (M=128 N=128 K=32, operands resident in shared memory):
     # a short burst before the timed region, and a sustained figure -- one launch of about
@@ -304,22 +347,23 @@ def run_ours(args):
     # ~100 ms launches back to back inside a long step, so the sustained figure is its ceiling.
     int8_sustained = mgx.peak_int8(1, 60_000_000)
     bf16_burst, bf16_sust, hbm, peak_kind = peaks()
-    pairs = splits * (splits + 1) // 2
+    products = moduli if crt else splits * (splits + 1) // 2
     kp = (n + 31) // 32 * 32
-    int8_ops = 2.0 * n * n * kp * pairs
+    int8_ops = 2.0 * n * n * kp * products
     gemm_avg_ms = sum(gemm_ms) / len(gemm_ms)
     achieved = int8_ops / (gemm_avg_ms * 1e-3) / 1e12
     peak = int8_sustained
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": OZAKI_GEMM_TRAFFIC_BYTES, "kernel": "ozaki_gemm",
+                "traffic": (CRT_GEMM_TRAFFIC_BYTES if crt else OZAKI_GEMM_TRAFFIC_BYTES) if n == N_DEFAULT else None,
+                "kernel": "crt_gemm" if crt else "ozaki_gemm",
                 "peak_note": (f"INT8 dense peak measured on this GPU by mgx_peak_int8 (tcgen05.mma kind::i8 "
                               f"128x128x32 loop): sustained over one ~2.5 s launch {int8_sustained:.0f} TOP/s (used), "
                               f"burst {int8_peak:.0f} TOP/s; 2 x the {peak_kind} bf16 cuBLAS burst would be "
                               f"{2 * bf16_burst:.0f}"),
                 "peak_burst": int8_peak, "frac_of_burst": achieved / int8_peak,
                 "frac_of_2x_bf16_burst": achieved / (2.0 * bf16_burst),
-                "ops_per_launch": int8_ops, "launch_ms": gemm_avg_ms,
-                "split_ms": ms_per_step - gemm_avg_ms}
+                "ops_per_launch": int8_ops, "int8_products": products, "launch_ms": gemm_avg_ms,
+                "other_kernels_ms": ms_per_step - gemm_avg_ms}
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -339,13 +383,17 @@ def run_ours(args):
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "TFLOP/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
 
-    launches_per_step = 6  # row_exp, col_max, col_exp, split_a, split_b, ozaki_gemm
+    # CRT: row_scale, col_max, col_sumsq, col_scale, split_a, split_b, crt_gemm, crt_combine;
+    # slices: row_exp, col_max, col_exp, split_a, split_b, ozaki_gemm
+    launches_per_step = 8 if crt else 6
     line = {
         "metric": METRIC, "value": value if valid else 0.0, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"dgemm_n{n}_wide_exp{EXP_RANGE}", "m": n, "n": n, "k": n, "form": "ozaki-int8",
-                   "splits": splits, "input": f"u*2^e, u~U[-1,1), e~U{{-{EXP_RANGE}..{EXP_RANGE}}}",
+        "config": {"workload": f"dgemm_n{n}_wide_exp{EXP_RANGE}", "m": n, "n": n, "k": n,
+                   "form": "ozaki-int8-crt" if crt else "ozaki-int8-slices",
+                   **({"moduli": moduli} if crt else {"splits": splits}),
+                   "input": f"u*2^e, u~U[-1,1), e~U{{-{EXP_RANGE}..{EXP_RANGE}}}",
                    "l2": "inputs larger than L2 (2 GiB per matrix vs 126 MB)", "error_gate": ERROR_GATE,
                    "per_rank": "independent product per GPU (weak scaling)"},
         "valid": bool(valid),
@@ -353,6 +401,7 @@ def run_ours(args):
                      "max_componentwise": err["max_componentwise"], "rows_checked": err["rows_checked"],
                      "reference": "double-double product on the GPU"},
         "native_fp64": native,
+        "ozaki_other_form": other or None,
         "speedup_vs_native_fp64": (value / native["tflops"]) if native else None,
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": launches_per_step * args.steps,
@@ -383,6 +432,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="matrix size (the metric is quoted at 16384)")
+    ap.add_argument("--form", choices=["crt", "slices"], default="crt",
+                    help="Ozaki form timed for `value`: CRT (scheme II, default) or digit slices")
+    ap.add_argument("--moduli", type=int, default=0, help="CRT moduli (0 = chosen for the 1e-15 gate)")
     ap.add_argument("--splits", type=int, default=0, help="Ozaki slices (0 = chosen for the 1e-15 gate)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--ref-step-seconds", type=float, default=8.0, help="reference arm: seconds per step")

@@ -41,7 +41,7 @@ extern "C" {
 #endif
 
 /* Arithmetic forms of the product. */
-typedef enum { MGX_FORM_FP64 = 0, MGX_FORM_OZAKI = 1 } mgx_form_t;
+typedef enum { MGX_FORM_FP64 = 0, MGX_FORM_OZAKI = 1, MGX_FORM_CRT = 2 } mgx_form_t;
 
 typedef enum {
     MGX_SUCCESS = 0,
@@ -176,6 +176,18 @@ MGX_API int mgx_gemm_ozaki_crt(const double *A, const double *B, double *C, int 
                                int ldb, int ldc, int beta_one, int moduli, void *workspace,
                                size_t workspace_bytes, void *stream);
 
+/* The three phases of mgx_gemm_ozaki_crt for one K range of at most mgx_crt_kmax(), each
+ * stream-ordered on the same workspace: mgx_crt_split writes the scales and residues of A and B;
+ * mgx_crt_products runs the residue products on the tensor cores (one persistent launch);
+ * mgx_crt_combine rebuilds C (+)= A B from the product residues.  Splitting once and
+ * multiplying several times reuses the residues. */
+MGX_API int mgx_crt_split(const double *A, const double *B, int m, int n, int k, int lda, int ldb, int moduli,
+                          void *workspace, size_t workspace_bytes, void *stream);
+MGX_API int mgx_crt_products(int m, int n, int k, int moduli, void *workspace, size_t workspace_bytes,
+                             void *stream);
+MGX_API int mgx_crt_combine(double *C, int m, int n, int k, int ldc, int beta_one, int moduli, void *workspace,
+                            size_t workspace_bytes, void *stream);
+
 /* Smallest modulus count whose a-priori normwise error bound meets `target` for reduction
  * length k (8..16). */
 MGX_API int mgx_crt_choose_moduli(int k, double target);
@@ -184,8 +196,9 @@ MGX_API int mgx_crt_choose_moduli(int k, double target);
 MGX_API int mgx_crt_kmax(void);
 
 /* C = A B from HOST buffers (hA m x k, hB k x n, hC m x n, row-major, leading dimensions in
- * elements) with form MGX_FORM_FP64 or MGX_FORM_OZAKI.  A is cut into `panels` (1..64) row panels
- * and B into `panels` column panels (multiples of 128); the panels are copied in the order A_0, B_0,
+ * elements) with form MGX_FORM_FP64, MGX_FORM_OZAKI (`splits` slices) or MGX_FORM_CRT (`splits` =
+ * moduli, 8..16).  A is cut into `panels` (1..64) row panels and B into `panels` column panels
+ * (multiples of 128; 256 for the CRT form); the panels are copied in the order A_0, B_0,
  * A_1, B_1, ... and every block (i, j) is computed as soon as A_i and B_j are on the device, then
  * copied back while the rest computes, so PCIe copies in both directions overlap the product.
  * The result is bit-identical to the device-buffer entry points'.  Device memory (A, B, C and

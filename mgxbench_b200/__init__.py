@@ -24,7 +24,7 @@ MGX_SUCCESS = 0
 STATUS_NAMES = {0: "success", -1: "invalid argument", -2: "CUDA error", -3: "non-finite input",
                 -4: "device-side wait timed out", -5: "workspace missing or too small",
                 -6: "unsupported configuration", -7: "device-side error"}
-FORM_FP64, FORM_OZAKI = 0, 1
+FORM_FP64, FORM_OZAKI, FORM_CRT = 0, 1, 2
 
 
 class MgxError(RuntimeError):
@@ -73,6 +73,9 @@ EXPORTS = [
     ("mgx_ozaki_kmax", _i, [_i]),
     ("mgx_crt_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_ozaki_crt", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_crt_split", _i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_crt_products", _i, [_i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_crt_combine", _i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_crt_choose_moduli", _i, [_i, _d]),
     ("mgx_crt_kmax", _i, []),
     ("mgx_gemm_ozaki_noalloc", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp]),
@@ -256,6 +259,29 @@ def gemm_ozaki_crt(A, B, C, moduli: int = 15, beta_one: bool = False, workspace=
     return _check(lib().mgx_gemm_ozaki_crt(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
                                            int(beta_one), moduli, _ptr(ws), ws.numel(), _stream(stream)),
                   "mgx_gemm_ozaki_crt")
+
+
+def crt_split(A, B, moduli: int, workspace, stream=None):
+    """Phase 1 of gemm_ozaki_crt (k <= crt_kmax()): scales and residues of A and B into `workspace`."""
+    _check_f64(A, B)
+    m, k = A.shape
+    n = B.shape[1]
+    return _check(lib().mgx_crt_split(_ptr(A), _ptr(B), m, n, k, _ld(A), _ld(B), moduli, _ptr(workspace),
+                                      workspace.numel(), _stream(stream)), "mgx_crt_split")
+
+
+def crt_products(m: int, n: int, k: int, moduli: int, workspace, stream=None):
+    """Phase 2: the residue products on the tensor cores (one persistent launch)."""
+    return _check(lib().mgx_crt_products(m, n, k, moduli, _ptr(workspace), workspace.numel(), _stream(stream)),
+                  "mgx_crt_products")
+
+
+def crt_combine(C, k: int, moduli: int, workspace, beta_one: bool = False, stream=None):
+    """Phase 3: C (+)= the CRT recombination of the product residues in `workspace`."""
+    _check_f64(C)
+    m, n = C.shape
+    return _check(lib().mgx_crt_combine(_ptr(C), m, n, k, _ld(C), int(beta_one), moduli, _ptr(workspace),
+                                        workspace.numel(), _stream(stream)), "mgx_crt_combine")
 
 
 def crt_choose_moduli(k: int, target: float = 1e-15) -> int:

@@ -1014,6 +1014,16 @@ extern "C" MGX_API int mgx_ozaki_kmax(int splits)
 int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                      int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic);
 
+// CRT form hooks (ozaki_crt.cu): whole-product workspace, panel preparation, block products.
+size_t mgx_crt_host_ws_bytes(int M, int N, int K, int q);
+int mgx_crt_host_rows(const double *A, int m, int lda, int r0, int M, int N, int K, int q, unsigned char *ws,
+                      cudaStream_t stream);
+int mgx_crt_host_cols(const double *B, int n, int ldb, int c0, int M, int N, int K, int q, unsigned char *ws,
+                      cudaStream_t stream);
+int mgx_crt_host_block(double *Cb, int ldc, int r0, int c0, int m, int n, int M, int N, int K, int q,
+                       unsigned char *ws, cudaStream_t stream);
+extern "C" MGX_API int mgx_crt_kmax(void);
+
 namespace {
 
 // Layout of rows [r0, ...) and columns [c0, ...) of a whole-problem workspace (r0, c0 multiples
@@ -1038,8 +1048,10 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
                                      int ldb, int ldc, int form, int splits, int panels, void *stream)
 {
     if (m < 0 || n < 0 || k < 0 || (m > 0 && n > 0 && (!hC || ldc < n)) ||
-        (m > 0 && n > 0 && k > 0 && (!hA || !hB || lda < k || ldb < n)) || (form != MGX_FORM_FP64 && form != MGX_FORM_OZAKI) ||
-        (form == MGX_FORM_OZAKI && (splits < 2 || splits > oz::MAX_SPLITS))) {
+        (m > 0 && n > 0 && k > 0 && (!hA || !hB || lda < k || ldb < n)) ||
+        (form != MGX_FORM_FP64 && form != MGX_FORM_OZAKI && form != MGX_FORM_CRT) ||
+        (form == MGX_FORM_OZAKI && (splits < 2 || splits > oz::MAX_SPLITS)) ||
+        (form == MGX_FORM_CRT && (splits < 8 || splits > 16))) {
         mgx_set_last_message("mgx_gemm_host: invalid arguments");
         return MGX_E_INVALID;
     }
@@ -1048,12 +1060,18 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
     if (panels < 1) panels = 1;
     if (panels > 64) panels = 64;  // 64 x 64 blocks at most: one event per block
     const bool ozaki = form == MGX_FORM_OZAKI && k > 0;
+    const bool crt = form == MGX_FORM_CRT && k > 0;
     if (ozaki && k > ozaki_kmax(splits)) {
         mgx_set_last_message("mgx_gemm_host: k = %d is above one int32 accumulation (%d) for %d splits", k,
                              ozaki_kmax(splits), splits);
         return MGX_E_UNSUPPORTED;
     }
-    const int prow = round_up((m + panels - 1) / panels, 128), pcol = round_up((n + panels - 1) / panels, 128);
+    if (crt && k > mgx_crt_kmax()) {
+        mgx_set_last_message("mgx_gemm_host: k = %d is above one int32 residue accumulation (%d)", k, mgx_crt_kmax());
+        return MGX_E_UNSUPPORTED;
+    }
+    const int align = crt ? 256 : 128;  // panels start on output tiles of the form
+    const int prow = round_up((m + panels - 1) / panels, align), pcol = round_up((n + panels - 1) / panels, align);
     const int Pm = (m + prow - 1) / prow, Pn = (n + pcol - 1) / pcol, T = Pm > Pn ? Pm : Pn;
     auto r_at = [&](int i) { return i * prow < m ? i * prow : m; };
     auto c_at = [&](int j) { return j * pcol < n ? j * pcol : n; };
@@ -1061,7 +1079,8 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
     const WsLayout L = ozaki ? ws_layout(m, n, k, splits) : WsLayout{};
     // device copies of A, B and C, then the Ozaki workspace of the whole product
     const size_t bA = align256((size_t)m * kk * sizeof(double)), bB = align256(kk * n * sizeof(double)),
-                 bC = align256((size_t)m * n * sizeof(double)), bW = ozaki ? L.total : 0;
+                 bC = align256((size_t)m * n * sizeof(double)),
+                 bW = ozaki ? L.total : (crt ? mgx_crt_host_ws_bytes(m, n, k, splits) : 0);
     char *mem = nullptr;
     {
         const int arc = mgx_scratch_alloc(reinterpret_cast<void **>(&mem), bA + bB + bC + bW, s0);
@@ -1123,6 +1142,8 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
         if (ozaki) {
             const WsLayout S = ws_sub(L, r0, c0, splits);
             rc = ozaki_multiply_impl(Cb, r1 - r0, c1 - c0, k, n, 0, splits, ws, S, cs);
+        } else if (crt) {
+            rc = mgx_crt_host_block(Cb, n, r0, c0, r1 - r0, c1 - c0, m, n, k, splits, ws, cs);
         } else {
             rc = mgx_launch_dgemm(dA + (size_t)r0 * kk, dB + c0, Cb, r1 - r0, c1 - c0, k, 0, k, k, (int)kk, n, n, 0, cs,
                                   0);
@@ -1143,12 +1164,20 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
                 rc = ozaki_split_a_impl(dA + (size_t)r0 * kk, r1 - r0, k, (int)kk, splits, ws, ws_sub(L, r0, 0, splits),
                                         s0);
             }
+            if (crt && rc == MGX_SUCCESS) {
+                const int r0 = r_at(t), r1 = r_at(t + 1);
+                rc = mgx_crt_host_rows(dA + (size_t)r0 * kk, r1 - r0, (int)kk, r0, m, n, k, splits, ws, s0);
+            }
         }
         if (t < Pn) {
             fail(cudaStreamWaitEvent(s0, evB[t], 0), "wait");
             if (ozaki && rc == MGX_SUCCESS) {
                 const int c0 = c_at(t), c1 = c_at(t + 1);
                 rc = ozaki_split_b_impl(dB + c0, c1 - c0, k, n, splits, ws, ws_sub(L, 0, c0, splits), s0);
+            }
+            if (crt && rc == MGX_SUCCESS) {
+                const int c0 = c_at(t), c1 = c_at(t + 1);
+                rc = mgx_crt_host_cols(dB + c0, c1 - c0, n, c0, m, n, k, splits, ws, s0);
             }
         }
         fail(cudaEventRecord(evS[t], s0), "record");

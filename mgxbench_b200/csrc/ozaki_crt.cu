@@ -25,7 +25,7 @@
 //   crt_row_scale   sigma per row of A (one warp per row, integer sum of squares)
 //   crt_col_max / crt_col_sumsq / crt_col_scale   tau per column of B (integer atomics)
 //   crt_split_a     residues of A as swizzled K-major 256-row slabs [modulus][tile][K block]
-//   crt_split_b     residues of B^T, transposed through shared memory, same layout
+//   crt_split_b     residues of B^T, same layout (thread per column, coalesced reads)
 //   crt_gemm        persistent tcgen05 kernel over (modulus, 256 x 256 tile) work items:
 //       warp 0      producer: one bulk copy per operand per stage (KPACK K blocks)
 //       warp 1      TMEM owner and MMA issuer: two M=128 N=256 K=32 kind::i8 MMAs per K block
@@ -53,11 +53,15 @@ constexpr int KB = 32;                 // bytes of K per MMA
 constexpr int SLAB = TILE * KB;        // 8 KiB: one operand, one K block
 constexpr int KPACK = MGX_CRT_KPACK;   // K blocks per pipeline stage
 constexpr int STAGE_BYTES = 2 * KPACK * SLAB;
-constexpr int STAGES = (192 * 1024) / STAGE_BYTES;
+constexpr int STAGES = (232448 - 1280) / STAGE_BYTES;   // 227 KiB of shared memory per CTA
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = (2 + EPI_WARPS) * 32;
 constexpr int NONFINITE = 0x7fffffff;
 constexpr int OUT_TILE_BYTES = TILE * TILE;   // one residue byte per output
+#ifndef MGX_CRT_RASTER
+#define MGX_CRT_RASTER 16
+#endif
+constexpr int RASTER = MGX_CRT_RASTER;
 
 static_assert(STAGES >= 2 && STAGES <= 8, "pipeline depth");
 
@@ -202,9 +206,12 @@ __global__ void crt_col_scale(const unsigned long long *__restrict__ colmax, con
 // ---------------------------------------------------------------- residue kernels
 // Residues of one value: x = rint(v 2^sg) (|x| < 2^63) is split exactly into xh 2^32 + xl
 // (xl in [0, 2^32)); for each modulus y = xh (2^32 mod p) + xl (|y| < 2^40, exact) and
-// r = y - p rint(y / p), exact, in [-(p-1)/2, (p-1)/2] for odd p, +-128 for 256.  rint(y / p)
-// is computed by adding 1.5 * 2^52 to the fused product y * (1/p): y / p is never within 2^-9 of
-// a half-integer for odd p, far above the error of 1/p.  The low byte of r + 1.5 * 2^52 is r.
+// r = y - p rint(y / p), in [-(p-1)/2, (p-1)/2] for odd p, +-128 for 256.  A double
+// 1.5 * 2^52 + z with |z| < 2^51 an integer holds z mod 2^32 in its low word, so
+//   Y = fma(xh, c, xl + 1.5 * 2^52)   (exact)      -> low word y mod 2^32
+//   t = fma(y, 1/p, 1.5 * 2^52)       (one rounding) -> low word rint(y / p): y / p is never
+//       within 2^-9 of a half-integer for odd p, far above the error of the rounded 1/p
+// and r = lo(Y) - p lo(t) in 32-bit arithmetic (r is small, so the wrap-around cancels).
 template <int Q>
 __device__ __forceinline__ void residues(double v, int sg, const Consts &K, uint8_t (&r)[Q])
 {
@@ -212,12 +219,13 @@ __device__ __forceinline__ void residues(double v, int sg, const Consts &K, uint
     const double x = rint(scale2(v, sg));
     const double xh = floor(__dmul_rn(x, 2.3283064365386963e-10));  // x * 2^-32
     const double xl = __fma_rn(-xh, 4294967296.0, x);
+    const double xlr = __dadd_rn(xl, kRound);
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
         const double y = __fma_rn(xh, K.c32[l], xl);
-        const double qd = __dsub_rn(__fma_rn(y, K.inv_p[l], kRound), kRound);
-        const double rr = __fma_rn(-qd, (double)c_moduli[l], y);
-        r[l] = (uint8_t)__double2loint(__dadd_rn(rr, kRound));
+        const double Y = __fma_rn(xh, K.c32[l], xlr);
+        const double t = __fma_rn(y, K.inv_p[l], kRound);
+        r[l] = (uint8_t)((uint32_t)__double2loint(Y) - (uint32_t)__double2loint(t) * (uint32_t)c_moduli[l]);
     }
 }
 
@@ -229,82 +237,84 @@ __device__ __forceinline__ size_t slab_offset(int tile, int kb, int kblocks, int
     return ((size_t)tile * kblocks + kb) * (size_t)SLAB + (size_t)r * 32 + (c ^ (((r >> 2) & 1) << 4));
 }
 
-// One warp per (8-row group, K block): lane -> row (lane / 4), 8 consecutive k (lane % 4).
+// Block: 64 rows of A x one 32-wide K block; warp w takes rows 8w..8w+7, lane -> row (lane / 4)
+// and 8 consecutive k (lane % 4), so four lanes read one 256-byte row segment and write the 32
+// residue bytes of that row, one 8-byte store each per modulus.
 template <int Q>
-__global__ void __launch_bounds__(256) crt_split_a(const double *__restrict__ A, int m, int k, int lda, int mp,
-                                                   int kblocks, const int *__restrict__ sg, uint8_t *__restrict__ ra,
-                                                   size_t mod_stride, const __grid_constant__ Consts K)
+__global__ void __launch_bounds__(256, 3) crt_split_a(const double *__restrict__ A, int m, int k, int lda, int mp,
+                                                      int kblocks, const int *__restrict__ sg, uint8_t *__restrict__ ra,
+                                                      size_t mod_stride, const __grid_constant__ Consts K)
 {
-    const int lane = threadIdx.x & 31;
-    const long long wpb = blockDim.x >> 5;
-    const long long items = (long long)(mp / 8) * kblocks;
-    for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < items; it += (long long)gridDim.x * wpb) {
-        const int ro = (int)(it / kblocks), kb = (int)(it % kblocks);
-        const int row = ro * 8 + (lane >> 2), kq = lane & 3;
-        const int k0 = kb * 32 + kq * 8;
-        int s = (row < m) ? sg[row] : 0;
-        const bool live = row < m && s != NONFINITE;
-        if (!live) s = 0;
-        unsigned long long packed[Q];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int kb = blockIdx.y;
+    const int row = blockIdx.x * 64 + warp * 8 + (lane >> 2), kq = lane & 3;
+    if (row >= mp) return;
+    const int k0 = kb * 32 + kq * 8;
+    int s = (row < m) ? sg[row] : 0;
+    const bool live = row < m && s != NONFINITE;
+    if (!live) s = 0;
+    unsigned long long packed[Q];
 #pragma unroll
-        for (int l = 0; l < Q; ++l) packed[l] = 0;
-        const double *arow = A + (size_t)(row < m ? row : 0) * lda;
+    for (int l = 0; l < Q; ++l) packed[l] = 0;
+    const double *arow = A + (size_t)(live ? row : 0) * lda;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int kk = k0 + j;
-            double v = (live && kk < k) ? __ldg(arow + kk) : 0.0;
-            if (!isfinite(v)) v = 0.0;
-            uint8_t r[Q];
-            residues<Q>(v, s, K, r);
+    for (int j = 0; j < 8; ++j) {
+        const int kk = k0 + j;
+        double v = (live && kk < k) ? __ldg(arow + kk) : 0.0;
+        if (!isfinite(v)) v = 0.0;
+        uint8_t r[Q];
+        residues<Q>(v, s, K, r);
 #pragma unroll
-            for (int l = 0; l < Q; ++l) packed[l] |= (unsigned long long)r[l] << (8 * j);
-        }
-        const size_t off = slab_offset(row / TILE, kb, kblocks, row % TILE, kq * 8);
-#pragma unroll
-        for (int l = 0; l < Q; ++l)
-            *reinterpret_cast<unsigned long long *>(ra + (size_t)l * mod_stride + off) = packed[l];
+        for (int l = 0; l < Q; ++l) packed[l] |= (unsigned long long)r[l] << (8 * j);
     }
+    const size_t off = slab_offset(row / TILE, kb, kblocks, row % TILE, kq * 8);
+#pragma unroll
+    for (int l = 0; l < Q; ++l)
+        *reinterpret_cast<unsigned long long *>(ra + (size_t)l * mod_stride + off) = packed[l];
 }
 
-// Block: 32 k x 128 columns of B through shared memory (coalesced reads along the columns),
-// written as residues of B^T (column j of B is row j % 256 of slab tile j / 256).
+// Block: 64 consecutive columns of B x one 32-wide K block.  Warp w takes 32 of the columns
+// (lane = column, so every load is one coalesced 256-byte row segment) and K quarter w % 4
+// (8 consecutive k).  The 8 residue bytes of each (column, quarter) go to their swizzled place
+// in a shared-memory copy of the block's slab rows; the 64 rows x 32 bytes of each modulus are
+// one contiguous 2 KiB run of the slab (column j of B is row j % 256 of slab tile j / 256),
+// written out with 16-byte stores.
 template <int Q>
-__global__ void __launch_bounds__(256) crt_split_b(const double *__restrict__ B, int k, int n, int ldb, int kblocks,
-                                                   const int *__restrict__ tu, uint8_t *__restrict__ rb,
-                                                   size_t mod_stride, const __grid_constant__ Consts K)
+__global__ void __launch_bounds__(256, 3) crt_split_b(const double *__restrict__ B, int k, int n, int ldb, int kblocks,
+                                                      const int *__restrict__ tu, uint8_t *__restrict__ rb,
+                                                      size_t mod_stride, const __grid_constant__ Consts K)
 {
-    __shared__ double tb[32][129];
-    const int n0 = blockIdx.x * 128, kb = blockIdx.y;
-    const int k0 = kb * 32;
-    for (int idx = threadIdx.x; idx < 32 * 128; idx += 256) {
-        const int kk = idx >> 7, c = idx & 127;
-        double v = (k0 + kk < k && n0 + c < n) ? __ldg(B + (size_t)(k0 + kk) * ldb + n0 + c) : 0.0;
+    __shared__ __align__(16) unsigned char st[Q][64 * 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kb = blockIdx.y, kq = warp & 3;
+    const int rl = (warp >> 2) * 32 + lane;          // row of the block's 64
+    const int col = blockIdx.x * 64 + rl;
+    int s = (col < n) ? tu[col] : 0;
+    const bool live = col < n && s != NONFINITE;
+    if (!live) s = 0;
+    const double *bcol = B + (live ? col : 0);
+    unsigned long long packed[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) packed[l] = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int kk = kb * 32 + kq * 8 + j;
+        double v = (live && kk < k) ? __ldg(bcol + (size_t)kk * ldb) : 0.0;
         if (!isfinite(v)) v = 0.0;
-        tb[kk][c] = v;
+        uint8_t rr[Q];
+        residues<Q>(v, s, K, rr);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) packed[l] |= (unsigned long long)rr[l] << (8 * j);
     }
+    const int soff = rl * 32 + ((kq * 8) ^ (((rl >> 2) & 1) << 4));
+#pragma unroll
+    for (int l = 0; l < Q; ++l) *reinterpret_cast<unsigned long long *>(&st[l][soff]) = packed[l];
     __syncthreads();
-#pragma unroll 1
-    for (int half = 0; half < 2; ++half) {
-        const int item = threadIdx.x + 256 * half;
-        const int r = item >> 2, kq = item & 3;   // column n0 + r of B
-        const int col = n0 + r;
-        int s = (col < n) ? tu[col] : 0;
-        const bool live = col < n && s != NONFINITE;
-        if (!live) s = 0;
-        unsigned long long packed[Q];
-#pragma unroll
-        for (int l = 0; l < Q; ++l) packed[l] = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            uint8_t rr[Q];
-            residues<Q>(live ? tb[kq * 8 + j][r] : 0.0, s, K, rr);
-#pragma unroll
-            for (int l = 0; l < Q; ++l) packed[l] |= (unsigned long long)rr[l] << (8 * j);
-        }
-        const size_t off = slab_offset(col / TILE, kb, kblocks, col % TILE, kq * 8);
-#pragma unroll
-        for (int l = 0; l < Q; ++l)
-            *reinterpret_cast<unsigned long long *>(rb + (size_t)l * mod_stride + off) = packed[l];
+    const int c0 = blockIdx.x * 64;
+    unsigned char *dst = rb + ((size_t)(c0 / TILE) * kblocks + kb) * (size_t)SLAB + (size_t)(c0 % TILE) * 32;
+    for (int idx = threadIdx.x; idx < Q * 128; idx += 256) {
+        const int l = idx >> 7, o = (idx & 127) * 16;
+        *reinterpret_cast<uint4 *>(dst + (size_t)l * mod_stride + o) = *reinterpret_cast<const uint4 *>(&st[l][o]);
     }
 }
 
@@ -373,24 +383,27 @@ __device__ __forceinline__ uint32_t mod_p(int32_t g, uint32_t p, uint32_t M)
 }
 
 struct GemmParams {
-    const uint8_t *ra, *rb;   // residue slabs [modulus][tile][K block][256 x 32 B]
-    uint8_t *rc;              // output residues [modulus][tile m][tile n][h][quarter][chunk][lane][16 B]
+    const uint8_t *ra, *rb;   // residue slabs [modulus][tile][K block][256 x 32 B], at the block's first tile
+    uint8_t *rc;              // output residues [modulus][tile row][tile column][64 KiB], at the block's first tile
     size_t ra_mod, rb_mod, rc_mod;
-    int tiles_m, tiles_n, kblocks, q;
+    int tiles_m, tiles_n;     // tiles of this block of the product
+    int rc_tile_ld;           // tiles per row of the residue planes (the whole product's)
+    int kblocks, q;
     int *status;
     uint32_t barrett[MAXQ];
 };
 
-// Work item w: modulus w / (tiles), then 8-tile-row groups sweeping the columns together.
+// Work item w: modulus w / (tiles), then groups of RASTER tile rows sweeping the columns
+// together (the group's rows of A stay in L2 while each column tile of B is read once per group).
 __device__ __forceinline__ void item_of(const GemmParams &p, int w, int &l, int &tm, int &tn)
 {
     const int per = p.tiles_m * p.tiles_n;
     l = w / per;
     const int t = w - l * per;
-    const int per_group = 8 * p.tiles_n;
+    const int per_group = RASTER * p.tiles_n;
     const int g = t / per_group, r = t % per_group;
-    const int first = g * 8;
-    const int gsize = min(p.tiles_m - first, 8);
+    const int first = g * RASTER;
+    const int gsize = min(p.tiles_m - first, RASTER);
     tm = first + r % gsize;
     tn = r / gsize;
 }
@@ -525,8 +538,8 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             int l, tm, tn;
             item_of(p, w, l, tm, tn);
             const uint32_t pm = (uint32_t)c_moduli[l], M = p.barrett[l];
-            uint8_t *dst = p.rc + (size_t)l * p.rc_mod + ((size_t)tm * p.tiles_n + tn) * OUT_TILE_BYTES +
-                           (size_t)((h * 4 + qd) * 16) * 512 + lane * 16;
+            uint8_t *dst = p.rc + (size_t)l * p.rc_mod + ((size_t)tm * p.rc_tile_ld + tn) * OUT_TILE_BYTES +
+                           (size_t)((h * 4 + qd) * 32) * 256 + lane * 8;
             const uint32_t tbase = tmem_base + ((uint32_t)(32 * qd) << 16) + h * 256;
 #pragma unroll 1
             for (int c = 0; c < 8; ++c) {
@@ -539,8 +552,9 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
                     pk[j] = mod_p((int32_t)r[4 * j], pm, M) | (mod_p((int32_t)r[4 * j + 1], pm, M) << 8) |
                             (mod_p((int32_t)r[4 * j + 2], pm, M) << 16) | (mod_p((int32_t)r[4 * j + 3], pm, M) << 24);
                 }
-                *reinterpret_cast<uint4 *>(dst + (size_t)(2 * c) * 512) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                *reinterpret_cast<uint4 *>(dst + (size_t)(2 * c + 1) * 512) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    *reinterpret_cast<uint2 *>(dst + (size_t)(4 * c + u) * 256) = make_uint2(pk[2 * u], pk[2 * u + 1]);
             }
             tc_fence_before();
             __syncwarp();
@@ -556,42 +570,44 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
 }
 
 // ---------------------------------------------------------------- CRT recombination
-// One warp per (tile, h, quarter, 16-column chunk): lane = row within the quarter, 16 columns.
-// beta_one: C (+)= result.
+// Product residues of one 256 x 256 tile are stored [h][quarter][8-column chunk][lane][8 B]: the
+// epilogue warp of TMEM lane quarter `quarter` and accumulator h writes 256 contiguous bytes per
+// chunk.  One warp here takes one (tile, h, quarter, chunk): lane = row within the quarter,
+// 8 columns.  beta_one: C (+)= result.
 struct CombineParams {
-    const uint8_t *rc;
+    const uint8_t *rc;        // the block's first tile of the residue planes
     size_t rc_mod;
-    double *C;
-    int m, n, ldc, tiles_n, beta_one, vec_store;
+    double *C;                // the block's first element of C
+    int m, n, ldc, tiles_n, rc_tile_ld, beta_one, vec_store;
     const int *sg, *tu;
     Consts K;
 };
 
 template <int Q>
-__global__ void __launch_bounds__(256) crt_combine(const __grid_constant__ CombineParams p, long long units)
+__global__ void __launch_bounds__(256, 3) crt_combine(const __grid_constant__ CombineParams p, long long units)
 {
     const int lane = threadIdx.x & 31;
     const long long unit = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (unit >= units) return;
-    const int c = (int)(unit & 15), qd = (int)((unit >> 4) & 3), h = (int)((unit >> 6) & 1);
-    const long long tile = unit >> 7;
+    const int c = (int)(unit & 31), qd = (int)((unit >> 5) & 3), h = (int)((unit >> 7) & 1);
+    const long long tile = unit >> 8;
     const int tm = (int)(tile / p.tiles_n), tn = (int)(tile % p.tiles_n);
     const int row = tm * TILE + h * 128 + qd * 32 + lane;
-    const int col0 = tn * TILE + c * 16;
+    const int col0 = tn * TILE + c * 8;
     if (row >= p.m || col0 >= p.n) return;
-    const uint8_t *src = p.rc + (size_t)tile * OUT_TILE_BYTES + (size_t)((h * 4 + qd) * 16 + c) * 512 + lane * 16;
-    double s1[16], s2[16], s3[16];
+    const uint8_t *src = p.rc + ((size_t)tm * p.rc_tile_ld + tn) * OUT_TILE_BYTES +
+                         (size_t)((h * 4 + qd) * 32 + c) * 256 + lane * 8;
+    double s1[8], s2[8], s3[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) s1[j] = s2[j] = s3[j] = 0.0;
+    for (int j = 0; j < 8; ++j) s1[j] = s2[j] = s3[j] = 0.0;
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src + (size_t)l * p.rc_mod));
-        const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+        const uint2 v = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)l * p.rc_mod));
         const double w1 = p.K.w[l][0], w2 = p.K.w[l][1], w3 = p.K.w[l][2];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < 8; ++j) {
             // (double) of one byte: 2^52 + b from the bit pattern, minus 2^52 (exact)
-            const double r = __dsub_rn(__hiloint2double(0x43300000, (wv[j >> 2] >> (8 * (j & 3))) & 255u),
+            const double r = __dsub_rn(__hiloint2double(0x43300000, ((j < 4 ? v.x : v.y) >> (8 * (j & 3))) & 255u),
                                        4503599627370496.0);
             s1[j] = __fma_rn(w1, r, s1[j]);
             s2[j] = __fma_rn(w2, r, s2[j]);
@@ -601,7 +617,7 @@ __global__ void __launch_bounds__(256) crt_combine(const __grid_constant__ Combi
     const int srow = p.sg[row];
     double *crow = p.C + (size_t)row * p.ldc;
 #pragma unroll
-    for (int j = 0; j < 16; j += 2) {
+    for (int j = 0; j < 8; j += 2) {
         double v[2];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
@@ -748,8 +764,9 @@ struct SplitA {
     static int run(const double *A, int m, int k, int lda, const CrtLayout &L, const int *sg, uint8_t *ra,
                    const crt::Consts &K, cudaStream_t stream)
     {
-        crt::crt_split_a<Q><<<mgx_sm_count() * 16, 256, 0, stream>>>(A, m, k, lda, L.tiles_m * crt::TILE, L.kblocks, sg,
-                                                                     ra, L.ra_mod, K);
+        const int tiles = (m + crt::TILE - 1) / crt::TILE;
+        crt::crt_split_a<Q><<<dim3(tiles * 4, L.kblocks), 256, 0, stream>>>(A, m, k, lda, tiles * crt::TILE,
+                                                                            L.kblocks, sg, ra, L.ra_mod, K);
         MGX_HOST_CHECK(cudaGetLastError());
         return MGX_SUCCESS;
     }
@@ -760,8 +777,9 @@ struct SplitB {
     static int run(const double *B, int n, int k, int ldb, const CrtLayout &L, const int *tu, uint8_t *rb,
                    const crt::Consts &K, cudaStream_t stream)
     {
-        crt::crt_split_b<Q><<<dim3(L.tiles_n * 2, L.kblocks), 256, 0, stream>>>(B, k, n, ldb, L.kblocks, tu, rb,
-                                                                                L.rb_mod, K);
+        const int tiles = (n + crt::TILE - 1) / crt::TILE;
+        crt::crt_split_b<Q><<<dim3(tiles * 4, L.kblocks), 256, 0, stream>>>(B, k, n, ldb, L.kblocks, tu, rb, L.rb_mod,
+                                                                            K);
         MGX_HOST_CHECK(cudaGetLastError());
         return MGX_SUCCESS;
     }
@@ -778,18 +796,32 @@ struct Combine {
     }
 };
 
-// Scale exponents and residues of A (m x k) and B (k x n), k <= KMAX.
-int crt_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, const crt::Consts &K,
-                   unsigned char *ws, const CrtLayout &L, cudaStream_t stream)
+// Scale exponents and residues of rows [r0, r0 + m) of A (m x k, k <= KMAX; r0 a multiple of
+// 256) into the whole-problem workspace.
+int crt_split_a_impl(const double *A, int m, int k, int lda, int r0, const crt::Consts &K, unsigned char *ws,
+                     const CrtLayout &L, cudaStream_t stream)
 {
+    if (m <= 0) return MGX_SUCCESS;
     int *status = mgx_device_status_ptr();
-    int *sg = reinterpret_cast<int *>(ws + L.sg);
-    int *tu = reinterpret_cast<int *>(ws + L.tu);
-    unsigned long long *colmax = reinterpret_cast<unsigned long long *>(ws + L.colmax);
-    unsigned long long *colsum = reinterpret_cast<unsigned long long *>(ws + L.colsum);
+    int *sg = reinterpret_cast<int *>(ws + L.sg) + r0;
+    uint8_t *ra = ws + L.ra + (size_t)(r0 / crt::TILE) * L.kblocks * crt::SLAB;
     crt::crt_row_scale<<<(m + 7) / 8, 256, 0, stream>>>(A, m, k, lda, K.alpha, sg, status);
     MGX_HOST_CHECK(cudaGetLastError());
-    MGX_HOST_CHECK(cudaMemsetAsync(colmax, 0, 2 * align256(sizeof(unsigned long long) * (size_t)n), stream));
+    return dispatch_q<SplitA>(K.q, A, m, k, lda, L, (const int *)sg, ra, K, stream);
+}
+
+// The same for columns [c0, c0 + n) of B (k x n).
+int crt_split_b_impl(const double *B, int n, int k, int ldb, int c0, const crt::Consts &K, unsigned char *ws,
+                     const CrtLayout &L, cudaStream_t stream)
+{
+    if (n <= 0) return MGX_SUCCESS;
+    int *status = mgx_device_status_ptr();
+    int *tu = reinterpret_cast<int *>(ws + L.tu) + c0;
+    unsigned long long *colmax = reinterpret_cast<unsigned long long *>(ws + L.colmax) + c0;
+    unsigned long long *colsum = reinterpret_cast<unsigned long long *>(ws + L.colsum) + c0;
+    uint8_t *rb = ws + L.rb + (size_t)(c0 / crt::TILE) * L.kblocks * crt::SLAB;
+    MGX_HOST_CHECK(cudaMemsetAsync(colmax, 0, sizeof(unsigned long long) * (size_t)n, stream));
+    MGX_HOST_CHECK(cudaMemsetAsync(colsum, 0, sizeof(unsigned long long) * (size_t)n, stream));
     const int sms = mgx_sm_count();
     int ych = (sms * 8) / ((n + 255) / 256);
     if (ych > (k + 63) / 64) ych = (k + 63) / 64;
@@ -800,31 +832,62 @@ int crt_split_impl(const double *A, const double *B, int m, int n, int k, int ld
     MGX_HOST_CHECK(cudaGetLastError());
     crt::crt_col_scale<<<(n + 255) / 256, 256, 0, stream>>>(colmax, colsum, n, K.beta, tu, status);
     MGX_HOST_CHECK(cudaGetLastError());
-    int rc = dispatch_q<SplitA>(K.q, A, m, k, lda, L, (const int *)sg, ws + L.ra, K, stream);
-    if (rc == MGX_SUCCESS) rc = dispatch_q<SplitB>(K.q, B, n, k, ldb, L, (const int *)tu, ws + L.rb, K, stream);
+    return dispatch_q<SplitB>(K.q, B, n, k, ldb, L, (const int *)tu, rb, K, stream);
+}
+
+int crt_split_impl(const double *A, const double *B, int m, int n, int k, int lda, int ldb, const crt::Consts &K,
+                   unsigned char *ws, const CrtLayout &L, cudaStream_t stream)
+{
+    int rc = crt_split_a_impl(A, m, k, lda, 0, K, ws, L, stream);
+    if (rc == MGX_SUCCESS) rc = crt_split_b_impl(B, n, k, ldb, 0, K, ws, L, stream);
     return rc;
 }
 
-// Residue products (tcgen05) and the CRT recombination into C.
-int crt_multiply_impl(double *C, int m, int n, int ldc, int beta_one, const crt::Consts &K, unsigned char *ws,
-                      const CrtLayout &L, cudaStream_t stream)
+// A block of the product inside a whole-problem workspace: rows [r0, r0 + m) and columns
+// [c0, c0 + n), r0 and c0 multiples of 256.
+struct CrtView {
+    const uint8_t *ra, *rb;
+    uint8_t *rc;
+    const int *sg, *tu;
+    int m, n, tiles_m, tiles_n;
+};
+
+CrtView crt_view(const CrtLayout &L, unsigned char *ws, int r0, int c0, int m, int n)
+{
+    CrtView v;
+    const int tm0 = r0 / crt::TILE, tn0 = c0 / crt::TILE;
+    v.ra = ws + L.ra + (size_t)tm0 * L.kblocks * crt::SLAB;
+    v.rb = ws + L.rb + (size_t)tn0 * L.kblocks * crt::SLAB;
+    v.rc = ws + L.rc + ((size_t)tm0 * L.tiles_n + tn0) * crt::OUT_TILE_BYTES;
+    v.sg = reinterpret_cast<const int *>(ws + L.sg) + r0;
+    v.tu = reinterpret_cast<const int *>(ws + L.tu) + c0;
+    v.m = m;
+    v.n = n;
+    v.tiles_m = (m + crt::TILE - 1) / crt::TILE;
+    v.tiles_n = (n + crt::TILE - 1) / crt::TILE;
+    return v;
+}
+
+// Residue products of a block on the tensor cores (one persistent launch).
+int crt_products_impl(const crt::Consts &K, const CrtLayout &L, const CrtView &v, cudaStream_t stream)
 {
     crt::GemmParams p;
     memset(&p, 0, sizeof p);
-    p.ra = ws + L.ra;
-    p.rb = ws + L.rb;
-    p.rc = ws + L.rc;
+    p.ra = v.ra;
+    p.rb = v.rb;
+    p.rc = v.rc;
     p.ra_mod = L.ra_mod;
     p.rb_mod = L.rb_mod;
     p.rc_mod = L.rc_mod;
-    p.tiles_m = L.tiles_m;
-    p.tiles_n = L.tiles_n;
+    p.tiles_m = v.tiles_m;
+    p.tiles_n = v.tiles_n;
+    p.rc_tile_ld = L.tiles_n;
     p.kblocks = L.kblocks;
     p.q = K.q;
     p.status = mgx_device_status_ptr();
     for (int l = 0; l < crt::MAXQ; ++l) p.barrett[l] = K.barrett[l];
     const int smem = crt::STAGES * crt::STAGE_BYTES + 1024 + 256;
-    const long long items = (long long)K.q * L.tiles_m * L.tiles_n;
+    const long long items = (long long)K.q * v.tiles_m * v.tiles_n;
     if (items <= 0) return MGX_SUCCESS;
     if (items > 0x7fffffffll) {
         mgx_set_last_message("mgx_gemm_ozaki_crt: product too large (%lld work items)", items);
@@ -835,23 +898,40 @@ int crt_multiply_impl(double *C, int m, int n, int ldc, int beta_one, const crt:
     MGX_HOST_CHECK(cudaFuncSetAttribute(crt::crt_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     crt::crt_gemm<<<grid, crt::THREADS, smem, stream>>>(p);
     MGX_HOST_CHECK(cudaGetLastError());
+    return MGX_SUCCESS;
+}
 
+// CRT recombination of a block into C (the block's first element; leading dimension ldc).
+int crt_combine_impl(double *C, int ldc, int beta_one, const crt::Consts &K, const CrtLayout &L, const CrtView &v,
+                     cudaStream_t stream)
+{
     crt::CombineParams cp;
     memset(&cp, 0, sizeof cp);
-    cp.rc = ws + L.rc;
+    cp.rc = v.rc;
     cp.rc_mod = L.rc_mod;
     cp.C = C;
-    cp.m = m;
-    cp.n = n;
+    cp.m = v.m;
+    cp.n = v.n;
     cp.ldc = ldc;
-    cp.tiles_n = L.tiles_n;
+    cp.tiles_n = v.tiles_n;
+    cp.rc_tile_ld = L.tiles_n;
     cp.beta_one = beta_one;
     cp.vec_store = ((ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
-    cp.sg = reinterpret_cast<const int *>(ws + L.sg);
-    cp.tu = reinterpret_cast<const int *>(ws + L.tu);
+    cp.sg = v.sg;
+    cp.tu = v.tu;
     cp.K = K;
-    const long long units = (long long)L.tiles_m * L.tiles_n * 128;
+    const long long units = (long long)v.tiles_m * v.tiles_n * 256;
+    if (units <= 0) return MGX_SUCCESS;
     return dispatch_q<Combine>(K.q, cp, units, stream);
+}
+
+int crt_multiply_impl(double *C, int m, int n, int ldc, int beta_one, const crt::Consts &K, unsigned char *ws,
+                      const CrtLayout &L, cudaStream_t stream)
+{
+    const CrtView v = crt_view(L, ws, 0, 0, m, n);
+    int rc = crt_products_impl(K, L, v, stream);
+    if (rc == MGX_SUCCESS) rc = crt_combine_impl(C, ldc, beta_one, K, L, v, stream);
+    return rc;
 }
 
 }  // namespace
@@ -894,6 +974,103 @@ int mgx_crt_run(const double *A, const double *B, double *C, int m, int n, int k
         if (rc != MGX_SUCCESS) return rc;
     }
     return MGX_SUCCESS;
+}
+
+static int crt_phase_check(int m, int n, int k, int moduli, const void *workspace, size_t workspace_bytes,
+                           const char *who, crt::Consts &K, CrtLayout &L)
+{
+    if (m < 0 || n < 0 || k < 0 || k > crt::KMAX || !crt::make_consts(moduli, K)) {
+        mgx_set_last_message("%s: invalid arguments m=%d n=%d k=%d (<= %d) moduli=%d (8..16)", who, m, n, k, crt::KMAX,
+                             moduli);
+        return MGX_E_INVALID;
+    }
+    L = crt_layout(m, n, k, moduli);
+    if (!workspace || workspace_bytes < L.total || (reinterpret_cast<uintptr_t>(workspace) & 255)) {
+        mgx_set_last_message("%s: workspace needs %zu bytes, 256-byte aligned (got %zu)", who, L.total, workspace_bytes);
+        return MGX_E_WORKSPACE;
+    }
+    return MGX_SUCCESS;
+}
+
+extern "C" MGX_API int mgx_crt_split(const double *A, const double *B, int m, int n, int k, int lda, int ldb,
+                                     int moduli, void *workspace, size_t workspace_bytes, void *stream)
+{
+    crt::Consts K;
+    CrtLayout L;
+    int rc = crt_phase_check(m, n, k, moduli, workspace, workspace_bytes, "mgx_crt_split", K, L);
+    if (rc != MGX_SUCCESS) return rc;
+    if ((m > 0 && k > 0 && (!A || lda < k)) || (n > 0 && k > 0 && (!B || ldb < n))) {
+        mgx_set_last_message("mgx_crt_split: invalid operand pointers or leading dimensions");
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0 || k == 0) return MGX_SUCCESS;
+    return crt_split_impl(A, B, m, n, k, lda, ldb, K, static_cast<unsigned char *>(workspace), L, (cudaStream_t)stream);
+}
+
+extern "C" MGX_API int mgx_crt_products(int m, int n, int k, int moduli, void *workspace, size_t workspace_bytes,
+                                        void *stream)
+{
+    crt::Consts K;
+    CrtLayout L;
+    int rc = crt_phase_check(m, n, k, moduli, workspace, workspace_bytes, "mgx_crt_products", K, L);
+    if (rc != MGX_SUCCESS) return rc;
+    if (m == 0 || n == 0 || k == 0) return MGX_SUCCESS;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    return crt_products_impl(K, L, crt_view(L, ws, 0, 0, m, n), (cudaStream_t)stream);
+}
+
+extern "C" MGX_API int mgx_crt_combine(double *C, int m, int n, int k, int ldc, int beta_one, int moduli,
+                                       void *workspace, size_t workspace_bytes, void *stream)
+{
+    crt::Consts K;
+    CrtLayout L;
+    int rc = crt_phase_check(m, n, k, moduli, workspace, workspace_bytes, "mgx_crt_combine", K, L);
+    if (rc != MGX_SUCCESS) return rc;
+    if (m > 0 && n > 0 && (!C || ldc < n)) {
+        mgx_set_last_message("mgx_crt_combine: invalid C or ldc");
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0) return MGX_SUCCESS;
+    if (k == 0) {
+        if (beta_one) return MGX_SUCCESS;
+        MGX_HOST_CHECK(cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)n * sizeof(double), m,
+                                         (cudaStream_t)stream));
+        return MGX_SUCCESS;
+    }
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    return crt_combine_impl(C, ldc, beta_one ? 1 : 0, K, L, crt_view(L, ws, 0, 0, m, n), (cudaStream_t)stream);
+}
+
+// Hooks for the host-buffer schedule (mgx_gemm_host in ozaki.cu): a workspace for the whole
+// M x N x K product (K <= KMAX), panels prepared as they arrive and blocks computed from them.
+size_t mgx_crt_host_ws_bytes(int M, int N, int K, int q) { return crt_layout(M, N, K, q).total; }
+
+int mgx_crt_host_rows(const double *A, int m, int lda, int r0, int M, int N, int K, int q, unsigned char *ws,
+                      cudaStream_t stream)
+{
+    crt::Consts C;
+    if (!crt::make_consts(q, C)) return MGX_E_INVALID;
+    return crt_split_a_impl(A, m, K, lda, r0, C, ws, crt_layout(M, N, K, q), stream);
+}
+
+int mgx_crt_host_cols(const double *B, int n, int ldb, int c0, int M, int N, int K, int q, unsigned char *ws,
+                      cudaStream_t stream)
+{
+    crt::Consts C;
+    if (!crt::make_consts(q, C)) return MGX_E_INVALID;
+    return crt_split_b_impl(B, n, K, ldb, c0, C, ws, crt_layout(M, N, K, q), stream);
+}
+
+int mgx_crt_host_block(double *Cb, int ldc, int r0, int c0, int m, int n, int M, int N, int K, int q,
+                       unsigned char *ws, cudaStream_t stream)
+{
+    crt::Consts C;
+    if (!crt::make_consts(q, C)) return MGX_E_INVALID;
+    const CrtLayout L = crt_layout(M, N, K, q);
+    const CrtView v = crt_view(L, ws, r0, c0, m, n);
+    int rc = crt_products_impl(C, L, v, stream);
+    if (rc == MGX_SUCCESS) rc = crt_combine_impl(Cb, ldc, 0, C, L, v, stream);
+    return rc;
 }
 
 extern "C" MGX_API int mgx_gemm_ozaki_crt(const double *A, const double *B, double *C, int m, int n, int k, int lda,

@@ -109,3 +109,38 @@ def test_crt_argument_errors(mgx):
         with pytest.raises(mgx.MgxError):
             mgx.gemm_ozaki_crt(A, A, A.clone(), moduli=q)
     assert mgx.crt_workspace_size(4, 4, 4, 7) == 0
+
+
+def test_crt_phases_reuse_residues(mgx, oracle):
+    """split once, then products + combine twice: same result, equal to the oracle."""
+    import torch
+    rng = np.random.default_rng(21)
+    m, n, k, q = 300, 520, 777, 15
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    ws = torch.empty(mgx.crt_workspace_size(m, n, k, q), dtype=torch.uint8, device="cuda")
+    mgx.crt_split(dev(A), dev(B), q, ws)
+    dC = torch.empty((m, n), dtype=torch.float64, device="cuda")
+    mgx.crt_products(m, n, k, q, ws)
+    mgx.crt_combine(dC, k, q, ws)
+    first = host(dC).copy()
+    mgx.crt_products(m, n, k, q, ws)
+    mgx.crt_combine(dC, k, q, ws)
+    assert np.array_equal(bits(first), bits(host(dC)))
+    assert np.array_equal(bits(first), bits(oracle.crt_gemm(A, B, q)))
+
+
+@pytest.mark.parametrize("m,n,k,panels", [(1000, 700, 900, 3), (512, 512, 256, 1), (300, 1100, 64, 8), (257, 255, 300, 2)])
+def test_crt_host_buffer_path_matches_device_path(mgx, m, n, k, panels):
+    """mgx_gemm_host with the CRT form (panels of 256 rows/columns prepared as they arrive, blocks
+    computed from them) gives the device path's result bit for bit."""
+    import torch
+    rng = np.random.default_rng(m + n + k)
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    hA, hB = torch.from_numpy(A).pin_memory(), torch.from_numpy(B).pin_memory()
+    hC = torch.empty((m, n), dtype=torch.float64).pin_memory()
+    mgx.gemm_host(hA, hB, hC, form=mgx.FORM_CRT, splits=15, panels=panels)
+    torch.cuda.synchronize()
+    dC = torch.empty((m, n), dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=15)
+    assert np.array_equal(bits(hC.numpy()), bits(host(dC)))
+    assert mgx.device_status() == 0
