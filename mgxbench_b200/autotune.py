@@ -8,7 +8,7 @@ predicts both runtime and error:
 
   * `RegressionModel` -- the method without the network, in the reference's spirit: per
     candidate, log runtime = a + b log(MNK) by least squares, and log10 error looked up by
-    (split count, exponent-range bucket).
+    (form, split count, exponent-range bucket).
   * `MlpModel` -- a 3-layer FP32 MLP (6 -> 64 -> 64 -> 2) over (log2 M, log2 N, log2 K,
     exponent range, tile id, split count), trained and evaluated on the GPU by the library's own
     CUDA kernels (mgx_mlp_gradients / mgx_mlp_adam_step / mgx_mlp_forward).
@@ -35,9 +35,14 @@ TILE_OZAKI_128 = 1     # Ozaki INT8 kernel, 128 x 128 output tiles over the whol
 TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16 = 2, 3, 4, 5
 # Ozaki INT8 kernel, 128 x 128 output tiles, K cut into 4 / 16 slices (split-K)
 TILE_OZAKI_K4, TILE_OZAKI_K16 = 6, 7
+# CRT form (Ozaki scheme II), 256 x 256 output tiles over the whole K range; its "splits" is the
+# modulus count
+TILE_CRT = 8
 FP64_KSPLIT = {TILE_FP64: 1, TILE_FP64_K2: 2, TILE_FP64_K4: 4, TILE_FP64_K8: 8, TILE_FP64_K16: 16}
 OZAKI_KSPLIT = {TILE_OZAKI_128: 1, TILE_OZAKI_K4: 4, TILE_OZAKI_K16: 16}
 SPLITS = tuple(range(3, 10))
+CRT_MODULI = (9, 11, 12, 13, 14, 15, 16)
+CRT_KMAX = 130816
 ERROR_FLOOR = 1e-17
 
 
@@ -51,12 +56,20 @@ class Candidate:
         return self.tile in FP64_KSPLIT
 
     @property
+    def is_crt(self) -> bool:
+        return self.tile == TILE_CRT
+
+    @property
+    def form(self) -> str:
+        return "fp64" if self.is_fp64 else ("crt" if self.is_crt else "ozaki")
+
+    @property
     def ksplit(self) -> int:
         return FP64_KSPLIT.get(self.tile) or OZAKI_KSPLIT.get(self.tile, 1)
 
     @property
     def name(self) -> str:
-        base = "fp64" if self.is_fp64 else f"ozaki{self.splits}"
+        base = "fp64" if self.is_fp64 else f"{self.form}{self.splits}"
         return base if self.ksplit == 1 else f"{base}k{self.ksplit}"
 
 
@@ -83,8 +96,9 @@ def candidates(m=None, n=None, k=None):
     """Every configuration, or those that apply to an m x n x k product."""
     out = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16)]
     out += [Candidate(t, s) for t in (TILE_OZAKI_128, TILE_OZAKI_K4, TILE_OZAKI_K16) for s in SPLITS]
+    out += [Candidate(TILE_CRT, q) for q in CRT_MODULI]
     if m is not None:
-        out = [c for c in out if splitk_applies(m, n, k, c.ksplit, c.splits)]
+        out = [c for c in out if (k <= CRT_KMAX if c.is_crt else splitk_applies(m, n, k, c.ksplit, c.splits))]
     return out
 
 
@@ -114,6 +128,8 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
         def run():
             if c.is_fp64:
                 mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws)
+            elif c.is_crt:
+                mgx.gemm_ozaki_crt(A, B, C, moduli=c.splits, workspace=ws)
             else:
                 mgx.gemm_ozaki(A, B, C, splits=c.splits, workspace=ws, ksplit=c.ksplit)
         run()
@@ -125,7 +141,7 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
         e1.record()
         e1.synchronize()
         t = e0.elapsed_time(e1) / reps * 1e-3
-        key = (c.is_fp64, c.ksplit, c.splits)  # results depend on the form, K slices and split count only
+        key = (c.form, c.ksplit, c.splits)  # results depend on the form, K slices and split count only
         if key not in errors:
             rows = min(check_rows, m)
             errors[key] = mgx.error_vs_dd(A, B, C, row_start=(m - rows) // 2, row_count=rows)["normwise"]
@@ -170,10 +186,13 @@ def random_shapes(count, seed, lo=256, hi=32768, rmax=40):
     return [(int(a), int(b), int(c), int(r)) for (a, b, c), r in zip(dims, ranges)]
 
 
-def shape_fits(m, n, k, limit_bytes=60 * 2 ** 30):
-    """Keeps a measurement within a bounded share of device memory (A, B, C, the 9-slice Ozaki
-    workspace and at most SPLITK_WORKSPACE_LIMIT of split-K partial products)."""
-    return 8 * (m * k + k * n + m * n) + 9 * (m + n) * k + SPLITK_WORKSPACE_LIMIT < limit_bytes
+def shape_fits(m, n, k, limit_bytes=100 * 2 ** 30):
+    """Keeps a measurement within a bounded share of device memory (A, B, C and the largest
+    workspace: the 9-slice Ozaki one plus at most SPLITK_WORKSPACE_LIMIT of split-K partial
+    products, or the 16-modulus CRT one, residues of A, B and C rounded up to 256-row tiles)."""
+    r = lambda x: (x + 255) // 256 * 256
+    crt = 16 * (r(m) * k + r(n) * k + r(m) * r(n))
+    return 8 * (m * k + k * n + m * n) + max(9 * (m + n) * k + SPLITK_WORKSPACE_LIMIT, crt) < limit_bytes
 
 
 # ------------------------------------------------------------------ models
@@ -184,7 +203,7 @@ def _targets(rows):
 
 
 class RegressionModel:
-    """Per-candidate log-log runtime fit and a (splits, range bucket) error table."""
+    """Per-candidate log-log runtime fit and a (form, splits, range bucket) error table."""
 
     def fit(self, rows):
         self.rt = {}
@@ -201,7 +220,8 @@ class RegressionModel:
             self.rt[key] = (a, b)
         self.err = {}
         for r in rows:
-            self.err.setdefault((r["splits"], self._bucket(r["exp_range"])), []).append(
+            form = Candidate(r["tile"], r["splits"]).form
+            self.err.setdefault((form, r["splits"], self._bucket(r["exp_range"])), []).append(
                 math.log10(max(r["error"], ERROR_FLOOR)))
         self.err = {k: float(np.mean(v)) for k, v in self.err.items()}
         return self
@@ -215,9 +235,9 @@ class RegressionModel:
         for c in cands:
             a, b = self.rt.get((c.tile, c.splits), (0.0, 1.0))
             t = math.exp(a + b * math.log(m * n * k))
-            e = self.err.get((c.splits, self._bucket(exp_range)))
+            e = self.err.get((c.form, c.splits, self._bucket(exp_range)))
             if e is None:
-                near = [v for (s, bk), v in self.err.items() if s == c.splits]
+                near = [v for (f, s, bk), v in self.err.items() if f == c.form and s == c.splits]
                 e = float(np.mean(near)) if near else 0.0
             out.append((t, 10.0 ** e))
         return out
@@ -439,8 +459,7 @@ def main(argv=None):
         print(json.dumps(out, indent=1))
     elif a.cmd == "choose":
         c = choose(MlpModel.load(a.model), a.m, a.n, a.k, a.exp_range, a.target)
-        print(json.dumps({"form": "fp64" if c.is_fp64 else "ozaki", "tile": c.tile, "ksplit": c.ksplit,
-                          "splits": c.splits}))
+        print(json.dumps({"form": c.form, "tile": c.tile, "ksplit": c.ksplit, "splits": c.splits}))
     return 0
 
 

@@ -87,7 +87,7 @@ def cfg2():
             "max_rel_err": e["max_rel"], "rows_checked": e["rows_checked"]}
 
 
-def cfg3(splits=range(3, 10)):
+def cfg3(splits=range(3, 10), moduli=(12, 13, 14, 15, 16)):
     n, er = 16384, 20
     A, B, C = _mat(n, n, 2, 31, er), _mat(n, n, 2, 32, er), torch.empty((n, n), dtype=torch.float64, device="cuda")
     rows = (n // 2 - 128, 256)
@@ -102,6 +102,16 @@ def cfg3(splits=range(3, 10)):
         e = mgx.error_vs_dd(A, B, C, *rows)
         out.append({"config": "cfg3", "form": "ozaki", "splits": s, "n": n, "effective_tflops": 2 * n ** 3 / t / 1e12,
                     "seconds": t, "int8_tops": 2 * n ** 3 * s * (s + 1) / 2 / t / 1e12,
+                    "normwise_err": e["normwise"], "max_rel_err": e["max_rel"],
+                    "max_componentwise_err": e["max_componentwise"], "meets_1e-15": e["normwise"] <= 1e-15,
+                    "speedup_vs_fp64": tn / t})
+        del ws
+    for q in moduli:
+        ws = torch.empty(mgx.crt_workspace_size(n, n, n, q), dtype=torch.uint8, device="cuda")
+        t = _time(lambda: mgx.gemm_ozaki_crt(A, B, C, moduli=q, workspace=_Fixed(ws)), reps=2)
+        e = mgx.error_vs_dd(A, B, C, *rows)
+        out.append({"config": "cfg3", "form": "crt", "moduli": q, "n": n, "effective_tflops": 2 * n ** 3 / t / 1e12,
+                    "seconds": t, "int8_tops": 2 * n ** 3 * q / t / 1e12,
                     "normwise_err": e["normwise"], "max_rel_err": e["max_rel"],
                     "max_componentwise_err": e["max_componentwise"], "meets_1e-15": e["normwise"] <= 1e-15,
                     "speedup_vs_fp64": tn / t})
@@ -132,7 +142,7 @@ def cfg4(splits=None, model="default"):
             model = at.MlpModel.load(pr_mod.DEFAULT_MODEL) if pr_mod.DEFAULT_MODEL.is_file() else None
         if model is not None:
             plan_cands = [c for c in at.candidates() if c.ksplit == 1]  # SUMMA panels are the K split
-            oz = [c for c in plan_cands if not c.is_fp64]
+            oz = [c for c in plan_cands if c.form == "ozaki"]  # the plan runs the slice form
             splits = at.choose(model, M, N, K, 0, 1e-15, oz).splits
             chooser = "learned cost model"
     out = []
@@ -154,6 +164,23 @@ def cfg4(splits=None, model="default"):
                     "persistent_launches_per_product": 1, "splits_from": chooser if s else None})
         del g
         plan.close()
+    # the CRT form on the same grid: one whole-K product per block (exact integer sums, so the
+    # panel order does not matter), as build/mm_2d runs it with MGXBENCH_FORM=crt
+    q = mgx.crt_choose_moduli(K, 1e-15)
+    rcut = [M * i // pr for i in range(pr + 1)]
+    ccut = [N * j // pc for j in range(pc + 1)]
+    ws = mgx.OzakiWorkspace()
+
+    def blocks():
+        for i in range(pr):
+            for j in range(pc):
+                mgx.gemm_ozaki_crt(A[rcut[i]:rcut[i + 1]], B[:, ccut[j]:ccut[j + 1]],
+                                   C[rcut[i]:rcut[i + 1], ccut[j]:ccut[j + 1]], moduli=q, workspace=ws)
+    t = _time(blocks, reps=2)
+    e = mgx.error_vs_dd(A, B, C, row_start=M // 2 - 128, row_count=256)
+    out.append({"config": "cfg4", "form": "crt", "moduli": q, "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}",
+                "blocks": pr * pc, "tflops": 2 * M * N * K / t / 1e12, "seconds": t, "normwise_err": e["normwise"],
+                "max_rel_err": e["max_rel"], "graph": False, "moduli_from": "crt_choose_moduli"})
     return out
 
 

@@ -26,7 +26,7 @@
 namespace mm {
 
 struct AutoChoice {
-    int form = -1;        // MGX_FORM_FP64 or MGX_FORM_OZAKI
+    int form = -1;        // MGX_FORM_FP64, MGX_FORM_OZAKI or MGX_FORM_CRT
     int splits = 0;
     int ksplit = 1;       // FP64 split-K slices
     double predicted_s = 0.0;
@@ -80,7 +80,8 @@ inline std::string exe_dir()
 inline std::string default_model_path() { return exe_dir() + "/../mgxbench_b200/data/mlp_b200.json"; }
 
 // Tile ids of the candidates (mgxbench_b200.autotune): 0, 2, 3, 4, 5 are the FP64 kernel with
-// the K range cut into 1, 2, 4, 8, 16 slices; 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices.
+// the K range cut into 1, 2, 4, 8, 16 slices; 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices;
+// 8 is the CRT form (its "splits" is the modulus count).
 inline int tile_ksplit(int tile)
 {
     switch (tile) {
@@ -94,7 +95,8 @@ inline int tile_ksplit(int tile)
     }
 }
 
-inline bool tile_is_fp64(int tile) { return tile != 1 && tile != 6 && tile != 7; }
+inline bool tile_is_crt(int tile) { return tile == 8; }
+inline bool tile_is_fp64(int tile) { return tile != 1 && tile != 6 && tile != 7 && !tile_is_crt(tile); }
 
 // Same rule as mgxbench_b200.autotune.splitk_applies: each slice gets a 32-wide K block, the
 // partial products fit 4 GiB, and an Ozaki split needs K within one int32 accumulation.
@@ -132,17 +134,25 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
     }
     if (!json_numbers(text, "candidates", &cand) || cand.empty() || cand.size() % 2) {
         cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0};  // default list: FP64 (1..16 K slices), Ozaki 3..9 splits
-        for (int t : {1, 6, 7})                 // with 1, 4, 16 K slices
+        for (int t : {1, 6, 7})                 // with 1, 4, 16 K slices, CRT 9, 11..16 moduli
             for (int s = 3; s <= 9; ++s) {
                 cand.push_back(t);
                 cand.push_back(s);
             }
+        for (int q : {9, 11, 12, 13, 14, 15, 16}) {
+            cand.push_back(8);
+            cand.push_back(q);
+        }
     }
     {   // keep the candidates that apply to this product
         std::vector<double> keep;
         for (size_t c = 0; c + 1 < cand.size(); c += 2) {
             const int ks = tile_ksplit((int)cand[c]);
-            if (!splitk_applies(m, n, k, ks, (int)cand[c + 1]) || (whole_k_only && ks > 1)) continue;
+            if (tile_is_crt((int)cand[c])) {
+                if (k > mgx_crt_kmax()) continue;
+            } else if (!splitk_applies(m, n, k, ks, (int)cand[c + 1]) || (whole_k_only && ks > 1)) {
+                continue;
+            }
             keep.push_back(cand[c]);
             keep.push_back(cand[c + 1]);
         }
@@ -196,7 +206,8 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
             most = c;
     }
     const int pick = best >= 0 ? best : most;
-    out->form = tile_is_fp64((int)cand[2 * pick]) ? MGX_FORM_FP64 : MGX_FORM_OZAKI;
+    out->form = tile_is_crt((int)cand[2 * pick]) ? MGX_FORM_CRT
+                : tile_is_fp64((int)cand[2 * pick]) ? MGX_FORM_FP64 : MGX_FORM_OZAKI;
     out->splits = (int)cand[2 * pick + 1];
     out->ksplit = tile_ksplit((int)cand[2 * pick]);
     out->predicted_s = std::exp(Y[(size_t)pick * 2] * ystd[0] + ymean[0]);
@@ -232,10 +243,10 @@ inline void resolve_auto_form(int *form, int *splits, int *ksplit, std::string *
         fflush(stderr);
         exit(exit_code);
     }
-    *form = c.form == MGX_FORM_OZAKI ? 1 : 0;
-    *splits = c.form == MGX_FORM_OZAKI ? c.splits : 0;
+    *form = c.form == MGX_FORM_OZAKI ? 1 : (c.form == MGX_FORM_CRT ? 3 : 0);
+    *splits = c.form == MGX_FORM_FP64 ? 0 : c.splits;
     *ksplit = c.ksplit;
-    *form_name = c.form == MGX_FORM_OZAKI ? "ozaki" : "fp64";
+    *form_name = c.form == MGX_FORM_OZAKI ? "ozaki" : (c.form == MGX_FORM_CRT ? "crt" : "fp64");
     printf("mmb autotune: model=%s m=%d n=%d k=%d exp_range=%g target=%.3e choice=%s splits=%d ksplit=%d "
            "predicted_s=%.6e predicted_err=%.3e\n",
            path.c_str(), m, n, k, exp_range, target, form_name->c_str(), *splits, *ksplit, c.predicted_s,

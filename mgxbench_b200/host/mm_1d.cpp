@@ -64,7 +64,7 @@ int main(int argc, char *argv[])
     const int input = mm::input_kind(&input_name);
     int form = mm::compute_form(&form_name);
     if (input < 0 || form < 0) {
-        fprintf(stderr, "MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|auto\n");
+        fprintf(stderr, "MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|crt|auto\n");
         return EXIT_FAILURE;
     }
     mm::cuda_or_die(cudaSetDevice(deviceId), "cudaSetDevice", EXIT_FAILURE);
@@ -91,10 +91,12 @@ int main(int argc, char *argv[])
                           chunked ? std::min(pipeline_k_chunk, k) : k,
                           input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, EXIT_FAILURE, chunked);
     if (chunked) ksplit = 1;
+    if (form == mm::kCrt && !autotuned)
+        splits = mm::env_int("MGXBENCH_MODULI", mgx_crt_choose_moduli(chunked ? std::min(pipeline_k_chunk, k) : k, 1e-15));
+    if (form == mm::kCrt) ksplit = 1;
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
     printf("mmb one-GPU emulation: ranks=%d rows/rank=%d form=%s%s input=%s B-structure=%s", nRanks, mi,
-           form_name.c_str(), form == mm::kOzaki ? (std::string(" splits=") + std::to_string(splits)).c_str() : "",
-           input_name.c_str(), chunked ? "K-chunked" : "single");
+           form_name.c_str(), mm::form_count(form, splits).c_str(), input_name.c_str(), chunked ? "K-chunked" : "single");
     if (chunked) printf(" K-chunk=%d", pipeline_k_chunk);
     printf(" launches=%s\n", batched ? "one for all ranks" : "one per rank");
 
@@ -205,7 +207,7 @@ int main(int argc, char *argv[])
         const int v = mgx_validate_matrix_c(d_C, m, n, expected_C, 1.0e-9, 1.0e-12, myRank, 1, nullptr);
         all_valid = (v == 1);
     } else {
-        const double tol = autotuned ? mm::auto_target() : form == mm::kOzaki ? 1e-15 : 1e-12;
+        const double tol = autotuned ? mm::auto_target() : mm::int8_form(form) ? 1e-15 : 1e-12;
         all_valid = mm::report_accuracy(d_A, d_B, d_C, m, n, k, mm::env_int("MGXBENCH_CHECK_ROWS", 256), tol, &err);
     }
     if (dev_status != 0) {
@@ -217,7 +219,7 @@ int main(int argc, char *argv[])
            "form=%s tflops=%.3f input=%s",
            libs, matrix_size, nRanks, avg_time_execution, all_valid, loop_count, form_name.c_str(), tflops,
            input_name.c_str());
-    if (form == mm::kOzaki) printf(" splits=%d", splits);
+    printf("%s", mm::form_count(form, splits).c_str());
     if (ksplit > 1) printf(" ksplit=%d", ksplit);
     if (input != mm::kConst) printf(" norm_rel_err=%.3e max_rel_err=%.3e", err.normwise, err.max_rel);
     printf("\n");

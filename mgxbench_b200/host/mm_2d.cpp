@@ -106,13 +106,16 @@ int main(int argc, char **argv)
     std::string input_name, form_name;
     const int input = mm::input_kind(&input_name);
     int form = mm::compute_form(&form_name);
-    if (input < 0 || form < 0) fail("MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|auto");
+    if (input < 0 || form < 0) fail("MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|crt|auto");
     int splits = mm::env_int("MGXBENCH_SPLITS", 8);
     int ksplit = 1;  // the SUMMA panels are the K split
     const bool autotuned = form == mm::kAuto;
     mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, M, Ncols, K,
                           input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, 2, true);
-    const int persistent = mm::env_int("MGXBENCH_PERSISTENT", 1);
+    if (form == mm::kCrt && !autotuned) splits = mm::env_int("MGXBENCH_MODULI", mgx_crt_choose_moduli(K, 1e-15));
+    // the persistent SUMMA kernel runs the FP64 and digit-slice forms; the CRT form runs one
+    // whole-K product per block (exact integer sums, so the panel order does not matter)
+    const int persistent = form == mm::kCrt ? 0 : mm::env_int("MGXBENCH_PERSISTENT", 1);
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
 
     printf("SUMMA rectangular grid=%dx%d N=%d BK=%d library=%s ranks=%d pipeline=2\n", Pr, Pc, N, BK, lib, p);
@@ -125,7 +128,7 @@ int main(int argc, char **argv)
                ((double)mmax * nmax * sizeof(double) + 2.0 * panel_bytes) / gib);
         printf("2D one-GPU emulation: M=%d N=%d K=%d blocks=%dx%d%s form=%s input=%s panels=%d %s\n", M, Ncols, K, Pr,
                Pc, uneven ? " (uneven split)" : "", form_name.c_str(), input_name.c_str(), (K + BK - 1) / BK,
-               persistent ? "persistent" : "per-panel launches");
+               persistent ? "persistent" : (mm::int8_form(form) ? "whole-K block products" : "per-panel launches"));
     }
 
     double *dA = nullptr, *dB = nullptr, *dC = nullptr;
@@ -168,7 +171,7 @@ int main(int argc, char **argv)
         if (plan) return mgx_summa_run(plan, dA, K, dB, Ncols, dC, Ncols, stream);
         cudaError_t e = cudaMemsetAsync(dC, 0, (size_t)M * Ncols * sizeof(double), stream);
         if (e != cudaSuccess) return MGX_E_CUDA;
-        if (form == mm::kOzaki) {  // integer panel sums are exact: one K loop per block
+        if (mm::int8_form(form)) {  // integer panel sums are exact: one K loop per block
             for (int bi = 0; bi < Pr; ++bi)
                 for (int bj = 0; bj < Pc; ++bj) {
                     const int r0 = rcut[bi], c0 = ccut[bj];
@@ -246,7 +249,7 @@ int main(int argc, char **argv)
                     }
             }
     } else {
-        const double tol = autotuned ? mm::auto_target() : form == mm::kOzaki ? 1e-15 : 1e-12;
+        const double tol = autotuned ? mm::auto_target() : mm::int8_form(form) ? 1e-15 : 1e-12;
         valid = mm::report_accuracy(dA, dB, dC, M, Ncols, K, mm::env_int("MGXBENCH_CHECK_ROWS", 256), tol, &err);
     }
     if (dev_status != 0) {
@@ -257,7 +260,7 @@ int main(int argc, char **argv)
     printf("BENCHMARK_RESULT decomposition=2D library=%s size=%d ranks=%d seconds=%.9f valid=%d loops=1 grid=%dx%d "
            "form=%s tflops=%.3f m=%d n=%d k=%d bk=%d input=%s",
            lib, N, p, elapsed, valid, Pr, Pc, form_name.c_str(), tflops, M, Ncols, K, BK, input_name.c_str());
-    if (form == mm::kOzaki) printf(" splits=%d", splits);
+    printf("%s", mm::form_count(form, splits).c_str());
     if (input != mm::kConst) printf(" norm_rel_err=%.3e max_rel_err=%.3e", err.normwise, err.max_rel);
     printf("\n");
     fflush(stdout);

@@ -60,17 +60,31 @@ inline int input_kind(std::string *name)
     return -1;
 }
 
-// Compute forms (MGXBENCH_FORM): native FP64 tensor-core MMA, the Ozaki INT8 form, or "auto"
-// (the learned cost model picks one of the two and the split count, see autotune.h).
-enum Form { kFp64 = 0, kOzaki = 1, kAuto = 2 };
+// Compute forms (MGXBENCH_FORM): native FP64 tensor-core MMA, the Ozaki INT8 digit-slice form,
+// its CRT form (Ozaki scheme II, MGXBENCH_MODULI moduli), or "auto" (the learned cost model picks
+// the form and its split or modulus count, see autotune.h).
+enum Form { kFp64 = 0, kOzaki = 1, kAuto = 2, kCrt = 3 };
 
 inline int compute_form(std::string *name)
 {
     *name = env_str("MGXBENCH_FORM", "fp64");
     if (*name == "fp64") return kFp64;
     if (*name == "ozaki") return kOzaki;
+    if (*name == "crt") return kCrt;
     if (*name == "auto") return kAuto;
     return -1;
+}
+
+// The INT8 forms compute exact integer products (their results do not depend on how K is cut
+// into panels) and are validated against 1e-15.
+inline bool int8_form(int form) { return form == kOzaki || form == kCrt; }
+
+// " splits=s" / " moduli=q" for the logs of the INT8 forms, "" for FP64.
+inline std::string form_count(int form, int splits)
+{
+    if (form == kOzaki) return " splits=" + std::to_string(splits);
+    if (form == kCrt) return " moduli=" + std::to_string(splits);
+    return "";
 }
 
 inline void check_or_die(int rc, const char *what, int exit_code)
@@ -91,7 +105,7 @@ inline void cuda_or_die(cudaError_t e, const char *what, int exit_code)
     }
 }
 
-// Device workspace for the Ozaki form, grown on demand.
+// Device workspace for the INT8 forms, grown on demand.
 struct Workspace {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -112,7 +126,8 @@ struct Workspace {
     }
 };
 
-// One block multiply C (+)= A B of the selected form with `ksplit` K slices.
+// One block multiply C (+)= A B of the selected form with `ksplit` K slices (`splits` holds the
+// modulus count for the CRT form).
 inline int block_gemm(int form, int splits, int ksplit, Workspace &ws, const double *A, const double *B, double *C,
                       int m, int n, int k, int lda, int ldb, int ldc, int beta_one, cudaStream_t s)
 {
@@ -123,6 +138,12 @@ inline int block_gemm(int form, int splits, int ksplit, Workspace &ws, const dou
         return mgx_gemm_fp64_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one, ksplit, w, need, s);
     }
     if (form == kFp64) return mgx_gemm_fp64(A, B, C, m, n, k, lda, ldb, ldc, beta_one, s);
+    if (form == kCrt) {
+        const size_t need = mgx_crt_workspace_size(m, n, k, splits);
+        void *w = ws.get(need);
+        if (!w && need) return MGX_E_CUDA;
+        return mgx_gemm_ozaki_crt(A, B, C, m, n, k, lda, ldb, ldc, beta_one, splits, w, need, s);
+    }
     if (ksplit > 1) {
         const size_t need = mgx_ozaki_splitk_workspace_size(m, n, k, splits, ksplit);
         void *w = ws.get(need);

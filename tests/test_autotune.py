@@ -9,7 +9,8 @@ from mgxbench_b200 import autotune as at
 
 def synthetic_rows(shapes, seed=0):
     """A toy machine: FP64 at 30 TF/s with error 1e-15 * sqrt(K/1e3); Ozaki s at 4.5 POPS / (s(s+1)/2)
-    plus a 1 GB/s-per-byte split cost, error 10^(-8 - 2(s-4)) for wide ranges."""
+    plus a 1 GB/s-per-byte split cost, error 10^(-8 - 2(s-4)) for wide ranges; CRT with q moduli
+    at 4.5 POPS / q plus its residue traffic, error 2 sqrt(K/6) 2^(-(L-3)/2)."""
     rng = np.random.default_rng(seed)
     rows = []
     for (m, n, k, er) in shapes:
@@ -20,6 +21,11 @@ def synthetic_rows(shapes, seed=0):
                 tiles = math.ceil(m / 128) * math.ceil(n / 128)
                 t = f / 30e12 * max(1.0, 148 / tiles) / min(c.ksplit, max(1.0, 148 / tiles)) + 3e-6 * c.ksplit
                 e = 1e-15 * math.sqrt(k / 1e3 / c.ksplit)
+            elif c.is_crt:
+                L = sum(math.log2(p) for p in (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211,
+                                               199, 197, 193)[:c.splits])
+                t = f * c.splits / 4.5e15 + 12.0 * (m * k + k * n + m * n) / 3e12
+                e = max(2 * math.sqrt(k / 6) * 2.0 ** (-(math.floor(L) - 2) / 2), 5e-17)
             else:
                 t = f * c.splits * (c.splits + 1) / 2 / 4.5e15 + 8.0 * (m * k + k * n) / 3e12
                 e = max(10.0 ** (-8 - 2 * (c.splits - 4)) * (1 if er > 8 else 0.1), 5e-17)
@@ -33,16 +39,17 @@ def test_candidates_and_features():
     cs = at.candidates()
     assert cs[0].tile == at.TILE_FP64 and cs[0].splits == 0 and cs[0].ksplit == 1
     assert [c.ksplit for c in cs if c.is_fp64] == [1, 2, 4, 8, 16]
-    assert [c.splits for c in cs if not c.is_fp64 and c.ksplit == 1] == list(range(3, 10))
-    assert sorted({c.ksplit for c in cs if not c.is_fp64}) == [1, 4, 16]
-    assert len({c.name for c in cs}) == len(cs) == 5 + 3 * 7
+    assert [c.splits for c in cs if c.form == "ozaki" and c.ksplit == 1] == list(range(3, 10))
+    assert sorted({c.ksplit for c in cs if c.form == "ozaki"}) == [1, 4, 16]
+    assert [c.splits for c in cs if c.is_crt] == list(at.CRT_MODULI) and {c.ksplit for c in cs if c.is_crt} == {1}
+    assert len({c.name for c in cs}) == len(cs) == 5 + 3 * 7 + 7
     oz5 = next(c for c in cs if c.splits == 5)
     f = at.features(1024, 2048, 4096, 20, oz5)
     assert f[:3] == [10.0, 11.0, 12.0] and f[3:] == [20.0, 1.0, 5.0]
     # split-K candidates only where the K range has the blocks and the slices fit the workspace cap
     small = at.candidates(300, 300, 100)            # 4 K blocks
     assert [c.ksplit for c in small if c.is_fp64] == [1, 2, 4]
-    assert sorted({c.ksplit for c in small if not c.is_fp64}) == [1, 4]
+    assert sorted({c.ksplit for c in small if c.form == "ozaki"}) == [1, 4]
     big = at.candidates(32768, 32768, 32768)
     assert [c.ksplit for c in big if c.is_fp64] == [1] and {c.ksplit for c in big} == {1}
     # an Ozaki K slice needs K within one int32 accumulation
@@ -63,7 +70,9 @@ def test_regression_baseline_and_choice():
     held = synthetic_rows(at.random_shapes(60, seed=3))
     reg = at.RegressionModel().fit(train)
     c = at.choose(reg, 8192, 8192, 8192, 20, 1e-15)
-    assert c.tile == at.TILE_OZAKI_128 and c.splits in (8, 9)
+    assert c.tile == at.TILE_CRT and c.splits in (15, 16)
+    c = at.choose(reg, 8192, 8192, 8192, 20, 1e-15, [x for x in at.candidates(8192, 8192, 8192) if x.form == "ozaki"])
+    assert c.form == "ozaki" and c.splits in (8, 9)
     r = at.regret(reg, held, 1e-15)
     assert r["shapes"] == 60 and r["mean_regret"] >= 0.0
     # an oracle that knows the measurements has zero regret
