@@ -43,6 +43,10 @@ OZAKI_KSPLIT = {TILE_OZAKI_128: 1, TILE_OZAKI_K4: 4, TILE_OZAKI_K16: 16}
 SPLITS = tuple(range(3, 10))
 CRT_MODULI = (9, 11, 12, 13, 14, 15, 16)
 CRT_KMAX = 130816
+# A CRT candidate must predict an error this many times below the target: its error falls only
+# ~10x per added modulus and grows with sqrt(K), so predictions near a target need a guard band
+# (the slice form's falls ~100x per slice).  Same constant in host/autotune.h.
+CRT_ERROR_MARGIN = 1.5
 ERROR_FLOOR = 1e-17
 
 
@@ -313,17 +317,18 @@ class MlpModel:
         return mdl
 
 
-def choose(model, m, n, k, exp_range, target, cands=None, margin=1.0):
-    """Fastest candidate whose predicted error is <= target / margin (largest split count if none)."""
+def choose(model, m, n, k, exp_range, target, cands=None, margin=1.0, crt_margin=CRT_ERROR_MARGIN):
+    """Fastest candidate whose predicted error is <= target / margin (target / (margin
+    crt_margin) for the CRT form); the largest split count if none."""
     cands = cands or candidates(m, n, k)
     pred = model.predict(m, n, k, exp_range, cands)
-    ok = [(t, c) for (t, e), c in zip(pred, cands) if e * margin <= target]
+    ok = [(t, c) for (t, e), c in zip(pred, cands) if e * margin * (crt_margin if c.is_crt else 1.0) <= target]
     if ok:
         return min(ok, key=lambda x: x[0])[1]
     return max(cands, key=lambda c: (c.splits, -c.tile))
 
 
-def regret(model, sweep_rows, target, margin=1.0):
+def regret(model, sweep_rows, target, margin=1.0, crt_margin=CRT_ERROR_MARGIN):
     """Mean and max of t(chosen) / t(best feasible) - 1 over the shapes of an exhaustive sweep,
     and how many choices missed the accuracy target."""
     shapes = {}
@@ -336,7 +341,7 @@ def regret(model, sweep_rows, target, margin=1.0):
         if not feasible:
             continue
         best = min(r["seconds"] for r in feasible)
-        c = choose(model, m, n, k, er, target, cands, margin)
+        c = choose(model, m, n, k, er, target, cands, margin, crt_margin)
         r = next(x for x in rs if x["tile"] == c.tile and x["splits"] == c.splits)
         if r["error"] > target:
             misses += 1

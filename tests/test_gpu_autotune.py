@@ -45,7 +45,7 @@ def test_executable_auto_form_matches_python_choice(tmp_path, exe, n, er):
     if exe == "mm_2d":
         cands = [c for c in cands if c.ksplit == 1]
     c = at.choose(model, n, n, n, er, 1e-15, cands)
-    assert m.group(1) == ("fp64" if c.is_fp64 else "ozaki")
+    assert m.group(1) == c.form
     assert int(m.group(2)) == c.splits and int(m.group(3)) == c.ksplit
     rec = dict(x.split("=", 1) for x in re.findall(r"BENCHMARK_RESULT\s+([^\r\n]+)", r.stdout)[0].split())
     assert rec["form"] == m.group(1)
