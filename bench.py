@@ -39,10 +39,11 @@ EXP_RANGE = 20
 ERROR_GATE = 1e-15
 CHECK_ROWS = 256
 # DRAM bytes (read + write) per launch of the dominant kernel at N = 16384, from one-pass ncu
-# captures at full size: ozaki_gemm (s = 8, profiles/ozaki_gemm_n4096.md: 167.53 GB + 2.16 GB)
-# and crt_gemm (q = 15, profiles/crt_gemm_n16384.md).
+# captures (dram__bytes_read.sum + dram__bytes_write.sum) of bench.py at full size:
+# ozaki_gemm with s = 8 reads 167.53 GB and writes 2.16 GB; crt_gemm with q = 15 reads
+# 118.02 GB and writes 4.03 GB.
 OZAKI_GEMM_TRAFFIC_BYTES = 169.69e9
-CRT_GEMM_TRAFFIC_BYTES = None
+CRT_GEMM_TRAFFIC_BYTES = 122.05e9
 
 
 def env_rank():

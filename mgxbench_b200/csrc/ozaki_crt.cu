@@ -39,7 +39,7 @@
 #include "mgx_common.cuh"
 
 #ifndef MGX_CRT_KPACK
-#define MGX_CRT_KPACK 2
+#define MGX_CRT_KPACK 4
 #endif
 
 namespace mgx {

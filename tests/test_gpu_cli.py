@@ -52,6 +52,28 @@ def test_mm1d_ozaki_random_inputs():
     assert rec["valid"] == "1" and float(rec["norm_rel_err"]) <= 1e-15
 
 
+@pytest.mark.parametrize("exe,ranks,n,env", [("mm_1d", 2, 1024, {}), ("mm_1d", 3, 1536, {"MGXBENCH_BATCH": 0}),
+                                              ("mm_2d", 6, 1536, {}), ("mm_2d", 15, 1000, {"MGXBENCH_UNEVEN": 1})])
+def test_crt_form_random_inputs(exe, ranks, n, env):
+    """MGXBENCH_FORM=crt: the CRT form with the a-priori modulus count for the 1e-15 gate (1D: row
+    blocks; 2D: one whole-K product per block), checked against the double-double product."""
+    r = launch(exe, ranks, n, "MMM", MGXBENCH_FORM="crt", MGXBENCH_INPUT="wide", MGXBENCH_CHECK_ROWS=128,
+               MGXBENCH_INNER_LOOPS=1, **env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rec = parse_result(r.stdout)
+    assert rec["form"] == "crt" and 14 <= int(rec["moduli"]) <= 16
+    assert rec["valid"] == "1" and float(rec["norm_rel_err"]) <= 1e-15
+
+
+def test_crt_form_constant_validation():
+    """The reference's constant check (A = 1, B = 2) through the CRT form: C = 2N exactly."""
+    r = launch("mm_1d", 4, 2048, "MMM", MGXBENCH_FORM="crt", MGXBENCH_MODULI=12)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rec = parse_result(r.stdout)
+    assert rec["valid"] == "1" and rec["moduli"] == "12"
+    assert "Result             : PASS" in r.stdout
+
+
 @pytest.mark.parametrize("lib,ranks,env", [("MMM", 1, {}), ("NNN", 4, {}), ("SSS", 6, {"MGXBENCH_SUMMA_BK": 64}),
                                            ("YYY", 15, {"MGXBENCH_GRID_ROWS": 3, "MGXBENCH_GRID_COLS": 5,
                                                         "MGXBENCH_SUMMA_BK": 128})])
@@ -92,7 +114,8 @@ def test_inaccurate_result_is_invalid_with_nonzero_exit(exe, ranks, n, code, env
     assert rec["valid"] == "0" and float(rec["norm_rel_err"]) > 1e-12
 
 
-@pytest.mark.parametrize("lib,form", [("MMM", "fp64"), ("SSS", "fp64"), ("MMM", "ozaki"), ("XXX", "ozaki")])
+@pytest.mark.parametrize("lib,form", [("MMM", "fp64"), ("SSS", "fp64"), ("MMM", "ozaki"), ("XXX", "ozaki"),
+                                      ("MMM", "crt"), ("SSS", "crt")])
 def test_mm1d_batched_ranks_give_the_same_result(lib, form):
     """All ranks' row blocks in one launch (default) or rank by rank: every element comes out of
     the same arithmetic, so the accuracy record is identical to the last digit printed."""

@@ -168,3 +168,57 @@ def test_ozaki_splitk_restatement(oracle):
         assert e <= 2 * e1 + 1e-16
     with pytest.raises(ValueError):
         oracle.ozaki_gemm_splitk(np.zeros((2, 70000)), np.zeros((70000, 2)), 8, 2)
+
+
+# ------------------------------------------------------------------ CRT form (Ozaki scheme II)
+# The reference has no INT8 form, so nothing of its own pins this restatement; exact integer
+# arithmetic does: every step before the final FP64 rounding is integer work.
+CRT_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193)
+
+
+def _crt_exact(A, B, q, sg, tu):
+    """Scaled integers A' = rint(A 2^sigma), B' = rint(B 2^tau) (ties to even, exact rationals)
+    and the exact integer product C' = A' B'."""
+    Ai = [[round(Fraction(float(a)) * Fraction(2) ** int(s)) for a in row] for row, s in zip(A, sg)]
+    Bi = [[round(Fraction(float(B[kk, j])) * Fraction(2) ** int(tu[j])) for j in range(B.shape[1])]
+          for kk in range(B.shape[0])]
+    C = [[sum(Ai[i][kk] * Bi[kk][j] for kk in range(len(Bi))) for j in range(B.shape[1])] for i in range(len(Ai))]
+    return Ai, Bi, C
+
+
+@pytest.mark.parametrize("q,kind,er", [(15, "wide", 20), (12, "uniform", 0), (16, "wide", 35), (9, "wide", 5)])
+def test_crt_oracle_against_exact_integers(oracle, q, kind, er):
+    import math
+    rng = np.random.default_rng(q * 7 + er)
+    m, n, k = 7, 6, 150
+    A, B = rng_matrix(rng, (m, k), kind, er), rng_matrix(rng, (k, n), kind, er)
+    A[2] = 0.0
+    sg, tu, rc = oracle.crt_scales(A, B, q)
+    assert rc == 0
+    P = math.prod(CRT_MODULI[:q])
+    L = P.bit_length()
+    alpha, beta = (L - 3) // 2, L - 3 - (L - 3) // 2
+    # the scale puts every row / column 2-norm at or below 2^alpha / 2^beta
+    for i in range(m):
+        if np.any(A[i]):
+            assert sum((Fraction(float(a)) * Fraction(2) ** int(sg[i])) ** 2 for a in A[i]) <= Fraction(4) ** alpha
+    for j in range(n):
+        assert sum((Fraction(float(b)) * Fraction(2) ** int(tu[j])) ** 2 for b in B[:, j]) <= Fraction(4) ** beta
+    Ai, Bi, Cx = _crt_exact(A, B, q, sg, tu)
+    # residues: the symmetric residue of the exact scaled integer, modulus by modulus
+    ra, rb, _, _ = oracle.crt_residues(A, B, q)
+    for l, p in enumerate(CRT_MODULI[:q]):
+        sym = (lambda x: ((x + 128) % 256) - 128) if p == 256 else (lambda x: ((x + p // 2) % p) - p // 2)
+        assert all(int(ra[l, i, kk]) == sym(Ai[i][kk]) for i in range(m) for kk in range(k))
+        assert all(int(rb[l, j, kk]) == sym(Bi[kk][j]) for j in range(n) for kk in range(k))
+    # every exact product lies within a quarter of P (unique CRT reconstruction), and the FP64
+    # result is that integer scaled back, within the two roundings of the recombination
+    C = oracle.crt_gemm(A, B, q)
+    for i in range(m):
+        for j in range(n):
+            assert 4 * abs(Cx[i][j]) < P
+            exact = Fraction(Cx[i][j]) * Fraction(2) ** (-int(sg[i]) - int(tu[j]))
+            if exact == 0:
+                assert C[i, j] == 0.0
+            else:
+                assert abs(Fraction(float(C[i, j])) - exact) <= 2 * abs(exact) * Fraction(2) ** -53
