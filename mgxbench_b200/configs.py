@@ -165,7 +165,8 @@ def cfg4(splits=None, model="default"):
         del g
         plan.close()
     # the CRT form on the same grid: one whole-K product per block (exact integer sums, so the
-    # panel order does not matter), as build/mm_2d runs it with MGXBENCH_FORM=crt
+    # panel order does not matter; build/mm_2d with MGXBENCH_FORM=crt MGXBENCH_BATCH=0), and all
+    # blocks as one product (its default), bit-identical
     q = mgx.crt_choose_moduli(K, 1e-15)
     rcut = [M * i // pr for i in range(pr + 1)]
     ccut = [N * j // pc for j in range(pc + 1)]
@@ -178,9 +179,18 @@ def cfg4(splits=None, model="default"):
                                    C[rcut[i]:rcut[i + 1], ccut[j]:ccut[j + 1]], moduli=q, workspace=ws)
     t = _time(blocks, reps=2)
     e = mgx.error_vs_dd(A, B, C, row_start=M // 2 - 128, row_count=256)
+    per_block = C.clone()
     out.append({"config": "cfg4", "form": "crt", "moduli": q, "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}",
-                "blocks": pr * pc, "tflops": 2 * M * N * K / t / 1e12, "seconds": t, "normwise_err": e["normwise"],
-                "max_rel_err": e["max_rel"], "graph": False, "moduli_from": "crt_choose_moduli"})
+                "blocks": pr * pc, "launches": "one product per block", "tflops": 2 * M * N * K / t / 1e12,
+                "seconds": t, "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": False,
+                "moduli_from": "crt_choose_moduli"})
+    t = _time(lambda: mgx.gemm_ozaki_crt(A, B, C, moduli=q, workspace=ws), reps=2)
+    e = mgx.error_vs_dd(A, B, C, row_start=M // 2 - 128, row_count=256)
+    out.append({"config": "cfg4", "form": "crt", "moduli": q, "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}",
+                "blocks": pr * pc, "launches": "all blocks in one product", "tflops": 2 * M * N * K / t / 1e12,
+                "seconds": t, "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": False,
+                "bit_identical_to_per_block": bool(torch.equal(C.view(torch.int64), per_block.view(torch.int64))),
+                "moduli_from": "crt_choose_moduli"})
     return out
 
 

@@ -116,6 +116,10 @@ int main(int argc, char **argv)
     // the persistent SUMMA kernel runs the FP64 and digit-slice forms; the CRT form runs one
     // whole-K product per block (exact integer sums, so the panel order does not matter)
     const int persistent = form == mm::kCrt ? 0 : mm::env_int("MGXBENCH_PERSISTENT", 1);
+    // CRT form: every block's result depends only on its rows of A and columns of B (whole-row
+    // and whole-column scales, exact integer sums), so all blocks run as one product by default
+    // (MGXBENCH_BATCH=1), bit-identical to one product per block (MGXBENCH_BATCH=0)
+    const bool crt_batched = form == mm::kCrt && mm::env_int("MGXBENCH_BATCH", 1) != 0;
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
 
     printf("SUMMA rectangular grid=%dx%d N=%d BK=%d library=%s ranks=%d pipeline=2\n", Pr, Pc, N, BK, lib, p);
@@ -128,7 +132,9 @@ int main(int argc, char **argv)
                ((double)mmax * nmax * sizeof(double) + 2.0 * panel_bytes) / gib);
         printf("2D one-GPU emulation: M=%d N=%d K=%d blocks=%dx%d%s form=%s input=%s panels=%d %s\n", M, Ncols, K, Pr,
                Pc, uneven ? " (uneven split)" : "", form_name.c_str(), input_name.c_str(), (K + BK - 1) / BK,
-               persistent ? "persistent" : (mm::int8_form(form) ? "whole-K block products" : "per-panel launches"));
+               persistent ? "persistent"
+                          : (crt_batched ? "all blocks in one product"
+                                         : (mm::int8_form(form) ? "whole-K block products" : "per-panel launches")));
     }
 
     double *dA = nullptr, *dB = nullptr, *dC = nullptr;
@@ -171,6 +177,8 @@ int main(int argc, char **argv)
         if (plan) return mgx_summa_run(plan, dA, K, dB, Ncols, dC, Ncols, stream);
         cudaError_t e = cudaMemsetAsync(dC, 0, (size_t)M * Ncols * sizeof(double), stream);
         if (e != cudaSuccess) return MGX_E_CUDA;
+        if (crt_batched)
+            return mm::block_gemm(form, splits, 1, ws, dA, dB, dC, M, Ncols, K, K, Ncols, Ncols, 1, stream);
         if (mm::int8_form(form)) {  // integer panel sums are exact: one K loop per block
             for (int bi = 0; bi < Pr; ++bi)
                 for (int bj = 0; bj < Pc; ++bj) {

@@ -65,6 +65,21 @@ def test_crt_form_random_inputs(exe, ranks, n, env):
     assert rec["valid"] == "1" and float(rec["norm_rel_err"]) <= 1e-15
 
 
+@pytest.mark.parametrize("ranks,env", [(6, {}), (15, {"MGXBENCH_UNEVEN": 1})])
+def test_crt_form_2d_one_product_equals_block_products(ranks, env):
+    """mm_2d with the CRT form: all blocks as one product (default) and one product per block
+    (MGXBENCH_BATCH=0) give the same result, so the accuracy records match to the last digit."""
+    recs = []
+    for batch in (1, 0):
+        r = launch("mm_2d", ranks, 1000, "MMM", MGXBENCH_FORM="crt", MGXBENCH_INPUT="wide", MGXBENCH_BATCH=batch,
+                   MGXBENCH_CHECK_ROWS=1000, MGXBENCH_INNER_LOOPS=1, **env)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert ("all blocks in one product" if batch else "whole-K block products") in r.stdout
+        recs.append(parse_result(r.stdout))
+    assert recs[0]["valid"] == recs[1]["valid"] == "1"
+    assert recs[0]["norm_rel_err"] == recs[1]["norm_rel_err"] and recs[0]["max_rel_err"] == recs[1]["max_rel_err"]
+
+
 def test_crt_form_constant_validation():
     """The reference's constant check (A = 1, B = 2) through the CRT form: C = 2N exactly."""
     r = launch("mm_1d", 4, 2048, "MMM", MGXBENCH_FORM="crt", MGXBENCH_MODULI=12)

@@ -1,6 +1,7 @@
 """Randomised shapes (seeded): the Ozaki form (whole-K and split-K, every split count) is
 bit-identical to the oracle's restatement, and the native FP64 form (whole-K and split-K) stays
-within the any-order summation bound, on ragged m, n, k including odd leading dimensions."""
+within the any-order summation bound, on ragged m, n, k including odd leading dimensions.  The
+CRT form (every modulus count) is bit-identical to its restatement on ragged shapes."""
 import numpy as np
 import pytest
 
@@ -30,4 +31,25 @@ def test_random_shape(mgx, oracle, m, n, k, s, ks):
     mgx.gemm_fp64(dA, dB, dF, ksplit=ks)
     _, _, ab = oracle.gemm_dd(A, B)
     assert np.all(np.abs(host(dF) - oracle.ab_multiply(A, B)) <= 2 * gamma(max(k, 1)) * ab + 1e-300)
+    assert mgx.device_status() == 0
+
+
+CRT_CASES = []
+_rng2 = np.random.default_rng(2027)
+for _ in range(16):
+    CRT_CASES.append((int(_rng2.integers(1, 600)), int(_rng2.integers(1, 600)), int(_rng2.integers(1, 1500)),
+                      int(_rng2.integers(8, 17)), int(_rng2.choice([0, 5, 20, 40]))))
+
+
+@pytest.mark.parametrize("m,n,k,q,er", CRT_CASES)
+def test_random_shape_crt(mgx, oracle, m, n, k, q, er):
+    """The CRT form on ragged shapes (tiles of 256 partly filled, K not a multiple of 32) and
+    exponent spreads from none to 2^+-40: bit-identical to the oracle's restatement."""
+    import torch
+    rng = np.random.default_rng(m * 7919 + n * 104729 + k * 13 + q + er)
+    kind = "wide" if er else "uniform"
+    A, B = rng_matrix(rng, (m, k), kind, max(er, 1)), rng_matrix(rng, (k, n), kind, max(er, 1))
+    dC = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=q)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, q)))
     assert mgx.device_status() == 0
