@@ -30,7 +30,8 @@
 //       warp 0      producer: one bulk copy per operand per stage (KPACK K blocks)
 //       warp 1      TMEM owner and MMA issuer: two M=128 N=256 K=32 kind::i8 MMAs per K block
 //                   (rows 0-127 and 128-255), int32 accumulators in all 512 TMEM columns
-//       warps 2-9   epilogue: tcgen05.ld, exact Barrett reduction mod p_l, one byte per output
+//       warps 2-17  epilogue (16 warps, two per accumulator and TMEM lane quarter, 128 columns
+//                   each): tcgen05.ld, exact Barrett reduction mod p_l, one byte per output
 //   crt_combine     CRT recombination of the q residue planes, scaling, (C +) store
 // All waits are bounded (mgx_common.cuh); TMEM is always released before the CTA exits.
 #include <cstdio>
@@ -54,7 +55,13 @@ constexpr int SLAB = TILE * KB;        // 8 KiB: one operand, one K block
 constexpr int KPACK = MGX_CRT_KPACK;   // K blocks per pipeline stage
 constexpr int STAGE_BYTES = 2 * KPACK * SLAB;
 constexpr int STAGES = (232448 - 1280) / STAGE_BYTES;   // 227 KiB of shared memory per CTA
-constexpr int EPI_WARPS = 8;
+#ifndef MGX_CRT_EPI_WARPS
+#define MGX_CRT_EPI_WARPS 16
+#endif
+constexpr int EPI_WARPS = MGX_CRT_EPI_WARPS;   // 8 or 16: one or two warps per (accumulator, TMEM lane quarter)
+constexpr int COL_SPLIT = EPI_WARPS / 8;       // warps sharing the 256 columns of one accumulator's lane quarter
+constexpr int EPI_CHUNKS = 8 / COL_SPLIT;      // 32-column chunks each epilogue warp drains
+static_assert(EPI_WARPS == 8 || EPI_WARPS == 16, "epilogue warps");
 constexpr int THREADS = (2 + EPI_WARPS) * 32;
 constexpr int NONFINITE = 0x7fffffff;
 constexpr int OUT_TILE_BYTES = TILE * TILE;   // one residue byte per output
@@ -524,9 +531,10 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             mbar_wait_bounded(drain, 0, p.status, kDevTimeoutAcc);
         }
     } else {
-        // ------------------------------------------------------------ epilogue (warps 2..9)
+        // ------------------------------------------------------------ epilogue (warps 2..)
         const int qd = warp & 3;            // TMEM lane quarter this warp may access
-        const int h = (warp - 2) >> 2;      // accumulator: tile rows 0-127 or 128-255
+        const int h = ((warp - 2) >> 2) & 1;  // accumulator: tile rows 0-127 or 128-255
+        const int c0 = ((warp - 2) >> 3) * EPI_CHUNKS;  // first 32-column chunk of this warp
         uint32_t acc_phase = 0;
         for (int w = blockIdx.x; w < items; w += gridDim.x) {
             bool got = true;
@@ -541,20 +549,27 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             uint8_t *dst = p.rc + (size_t)l * p.rc_mod + ((size_t)tm * p.rc_tile_ld + tn) * OUT_TILE_BYTES +
                            (size_t)((h * 4 + qd) * 32) * 256 + lane * 8;
             const uint32_t tbase = tmem_base + ((uint32_t)(32 * qd) << 16) + h * 256;
+            // two 32-column loads in flight per wait, then their reduction and stores
 #pragma unroll 1
-            for (int c = 0; c < 8; ++c) {
-                uint32_t r[32];
-                tmem_ld32(tbase + c * 32, r);
+            for (int c = c0; c < c0 + EPI_CHUNKS; c += 2) {
+                uint32_t r[2][32];
+                tmem_ld32(tbase + c * 32, r[0]);
+                tmem_ld32(tbase + (c + 1) * 32, r[1]);
                 tmem_wait_ld();
-                uint32_t pk[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    pk[j] = mod_p((int32_t)r[4 * j], pm, M) | (mod_p((int32_t)r[4 * j + 1], pm, M) << 8) |
-                            (mod_p((int32_t)r[4 * j + 2], pm, M) << 16) | (mod_p((int32_t)r[4 * j + 3], pm, M) << 24);
+                for (int b = 0; b < 2; ++b) {
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        pk[j] = mod_p((int32_t)r[b][4 * j], pm, M) | (mod_p((int32_t)r[b][4 * j + 1], pm, M) << 8) |
+                                (mod_p((int32_t)r[b][4 * j + 2], pm, M) << 16) |
+                                (mod_p((int32_t)r[b][4 * j + 3], pm, M) << 24);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        *reinterpret_cast<uint2 *>(dst + (size_t)(4 * (c + b) + u) * 256) =
+                            make_uint2(pk[2 * u], pk[2 * u + 1]);
                 }
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    *reinterpret_cast<uint2 *>(dst + (size_t)(4 * c + u) * 256) = make_uint2(pk[2 * u], pk[2 * u + 1]);
             }
             tc_fence_before();
             __syncwarp();

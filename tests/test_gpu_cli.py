@@ -65,14 +65,14 @@ def test_crt_form_random_inputs(exe, ranks, n, env):
     assert rec["valid"] == "1" and float(rec["norm_rel_err"]) <= 1e-15
 
 
-@pytest.mark.parametrize("ranks,env", [(6, {}), (15, {"MGXBENCH_UNEVEN": 1})])
-def test_crt_form_2d_one_product_equals_block_products(ranks, env):
+@pytest.mark.parametrize("ranks,n,env", [(6, 1200, {}), (15, 1000, {"MGXBENCH_UNEVEN": 1})])
+def test_crt_form_2d_one_product_equals_block_products(ranks, n, env):
     """mm_2d with the CRT form: all blocks as one product (default) and one product per block
     (MGXBENCH_BATCH=0) give the same result, so the accuracy records match to the last digit."""
     recs = []
     for batch in (1, 0):
-        r = launch("mm_2d", ranks, 1000, "MMM", MGXBENCH_FORM="crt", MGXBENCH_INPUT="wide", MGXBENCH_BATCH=batch,
-                   MGXBENCH_CHECK_ROWS=1000, MGXBENCH_INNER_LOOPS=1, **env)
+        r = launch("mm_2d", ranks, n, "MMM", MGXBENCH_FORM="crt", MGXBENCH_INPUT="wide", MGXBENCH_BATCH=batch,
+                   MGXBENCH_CHECK_ROWS=n, MGXBENCH_INNER_LOOPS=1, **env)
         assert r.returncode == 0, r.stdout + r.stderr
         assert ("all blocks in one product" if batch else "whole-K block products") in r.stdout
         recs.append(parse_result(r.stdout))
