@@ -1021,7 +1021,7 @@ int mgx_crt_host_rows(const double *A, int m, int lda, int r0, int M, int N, int
 int mgx_crt_host_cols(const double *B, int n, int ldb, int c0, int M, int N, int K, int q, unsigned char *ws,
                       cudaStream_t stream);
 int mgx_crt_host_block(double *Cb, int ldc, int r0, int c0, int m, int n, int M, int N, int K, int q,
-                       unsigned char *ws, cudaStream_t stream);
+                       unsigned char *ws, cudaStream_t stream, int slot);
 extern "C" MGX_API int mgx_crt_kmax(void);
 
 namespace {
@@ -1143,7 +1143,7 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
             const WsLayout S = ws_sub(L, r0, c0, splits);
             rc = ozaki_multiply_impl(Cb, r1 - r0, c1 - c0, k, n, 0, splits, ws, S, cs);
         } else if (crt) {
-            rc = mgx_crt_host_block(Cb, n, r0, c0, r1 - r0, c1 - c0, m, n, k, splits, ws, cs);
+            rc = mgx_crt_host_block(Cb, n, r0, c0, r1 - r0, c1 - c0, m, n, k, splits, ws, cs, blk & 1);
         } else {
             rc = mgx_launch_dgemm(dA + (size_t)r0 * kk, dB + c0, Cb, r1 - r0, c1 - c0, k, 0, k, k, (int)kk, n, n, 0, cs,
                                   0);

@@ -27,7 +27,10 @@
 //   crt_split_a     residues of A as swizzled K-major 256-row slabs [modulus][tile][K block]
 //   crt_split_b     residues of B^T, same layout (thread per column, coalesced reads)
 //   crt_gemm        persistent tcgen05 kernel over (modulus, 256 x 256 tile) work items:
-//       warp 0      producer: one bulk copy per operand per stage (KPACK K blocks)
+//       warp 0      producer: one bulk copy per operand per stage (KPACK K blocks); at each new
+//                   work item it waits (at most 20 us) until every CTA has started its item, so
+//                   the CTAs that share an operand tile read it within microseconds of each
+//                   other and mostly from L2 (DRAM reads at N = 16384: 118 -> 48 GB per launch)
 //       warp 1      TMEM owner and MMA issuer: two M=128 N=256 K=32 kind::i8 MMAs per K block
 //                   (rows 0-127 and 128-255), int32 accumulators in all 512 TMEM columns
 //       warps 2-17  epilogue (16 warps, two per accumulator and TMEM lane quarter, 128 columns
@@ -41,6 +44,9 @@
 
 #ifndef MGX_CRT_KPACK
 #define MGX_CRT_KPACK 4
+#endif
+#ifndef MGX_CRT_LOCKSTEP
+#define MGX_CRT_LOCKSTEP 1
 #endif
 
 namespace mgx {
@@ -397,6 +403,7 @@ struct GemmParams {
     int rc_tile_ld;           // tiles per row of the residue planes (the whole product's)
     int kblocks, q;
     int *status;
+    unsigned int *sync;       // this launch's arrival counter (zeroed before the launch), or nullptr
     uint32_t barrett[MAXQ];
 };
 
@@ -462,6 +469,22 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
                 int l, tm, tn;
                 item_of(p, w, l, tm, tn);
+#if MGX_CRT_LOCKSTEP
+                // Soft lockstep: CTAs that share an operand tile read it from L2 only while they
+                // stay within a few microseconds of each other, so every producer waits at each
+                // new item until all CTAs have started theirs -- or 20 us, then goes on anyway.
+                // Nothing depends on it for correctness, so it cannot deadlock (two launches that
+                // share the GPU just wait out the 20 us).
+                if (p.sync) {
+                    atomicAdd(p.sync, 1u);
+                    const unsigned int target = (unsigned int)min((long long)(w / gridDim.x + 1) * gridDim.x,
+                                                                  (long long)items);
+                    const unsigned long long t0 = global_ns();
+                    while (*reinterpret_cast<volatile unsigned int *>(p.sync) < target &&
+                           global_ns() - t0 < 20000ull)
+                        __nanosleep(64);
+                }
+#endif
                 const uint8_t *ga = p.ra + (size_t)l * p.ra_mod + (size_t)tm * p.kblocks * SLAB;
                 const uint8_t *gb = p.rb + (size_t)l * p.rb_mod + (size_t)tn * p.kblocks * SLAB;
                 for (int kb0 = 0; kb0 < p.kblocks; kb0 += KPACK) {
@@ -718,7 +741,7 @@ namespace {
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct CrtLayout {
-    size_t ra, rb, rc, sg, tu, colmax, colsum, total;
+    size_t ra, rb, rc, sg, tu, colmax, colsum, sync, total;
     size_t ra_mod, rb_mod, rc_mod;
     int kblocks, tiles_m, tiles_n;
 };
@@ -751,6 +774,8 @@ CrtLayout crt_layout(int m, int n, int k, int q)
     off = align256(off + sizeof(unsigned long long) * (size_t)n);
     L.colsum = off;
     off = align256(off + sizeof(unsigned long long) * (size_t)n);
+    L.sync = off;                       // arrival counters of the products launches (two slots)
+    off = align256(off + 2 * sizeof(unsigned int));
     L.total = off;
     return L;
 }
@@ -884,7 +909,8 @@ CrtView crt_view(const CrtLayout &L, unsigned char *ws, int r0, int c0, int m, i
 }
 
 // Residue products of a block on the tensor cores (one persistent launch).
-int crt_products_impl(const crt::Consts &K, const CrtLayout &L, const CrtView &v, cudaStream_t stream)
+int crt_products_impl(const crt::Consts &K, const CrtLayout &L, const CrtView &v, cudaStream_t stream,
+                      unsigned int *sync = nullptr)
 {
     crt::GemmParams p;
     memset(&p, 0, sizeof p);
@@ -910,6 +936,10 @@ int crt_products_impl(const crt::Consts &K, const CrtLayout &L, const CrtView &v
     }
     const int sms = mgx_sm_count();
     const int grid = (long long)sms < items ? sms : (int)items;
+    if (sync) {
+        MGX_HOST_CHECK(cudaMemsetAsync(sync, 0, sizeof(unsigned int), stream));
+        p.sync = sync;
+    }
     MGX_HOST_CHECK(cudaFuncSetAttribute(crt::crt_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     crt::crt_gemm<<<grid, crt::THREADS, smem, stream>>>(p);
     MGX_HOST_CHECK(cudaGetLastError());
@@ -944,7 +974,7 @@ int crt_multiply_impl(double *C, int m, int n, int ldc, int beta_one, const crt:
                       const CrtLayout &L, cudaStream_t stream)
 {
     const CrtView v = crt_view(L, ws, 0, 0, m, n);
-    int rc = crt_products_impl(K, L, v, stream);
+    int rc = crt_products_impl(K, L, v, stream, reinterpret_cast<unsigned int *>(ws + L.sync));
     if (rc == MGX_SUCCESS) rc = crt_combine_impl(C, ldc, beta_one, K, L, v, stream);
     return rc;
 }
@@ -1031,7 +1061,8 @@ extern "C" MGX_API int mgx_crt_products(int m, int n, int k, int moduli, void *w
     if (rc != MGX_SUCCESS) return rc;
     if (m == 0 || n == 0 || k == 0) return MGX_SUCCESS;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
-    return crt_products_impl(K, L, crt_view(L, ws, 0, 0, m, n), (cudaStream_t)stream);
+    return crt_products_impl(K, L, crt_view(L, ws, 0, 0, m, n), (cudaStream_t)stream,
+                             reinterpret_cast<unsigned int *>(ws + L.sync));
 }
 
 extern "C" MGX_API int mgx_crt_combine(double *C, int m, int n, int k, int ldc, int beta_one, int moduli,
@@ -1077,13 +1108,13 @@ int mgx_crt_host_cols(const double *B, int n, int ldb, int c0, int M, int N, int
 }
 
 int mgx_crt_host_block(double *Cb, int ldc, int r0, int c0, int m, int n, int M, int N, int K, int q,
-                       unsigned char *ws, cudaStream_t stream)
+                       unsigned char *ws, cudaStream_t stream, int slot)
 {
     crt::Consts C;
     if (!crt::make_consts(q, C)) return MGX_E_INVALID;
     const CrtLayout L = crt_layout(M, N, K, q);
     const CrtView v = crt_view(L, ws, r0, c0, m, n);
-    int rc = crt_products_impl(C, L, v, stream);
+    int rc = crt_products_impl(C, L, v, stream, reinterpret_cast<unsigned int *>(ws + L.sync) + (slot & 1));
     if (rc == MGX_SUCCESS) rc = crt_combine_impl(Cb, ldc, 0, C, L, v, stream);
     return rc;
 }
