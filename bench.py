@@ -40,9 +40,9 @@ ERROR_GATE = 1e-15
 CHECK_ROWS = 256
 # DRAM bytes (read + write) per launch of the dominant kernel at N = 16384, from one-pass ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum) of bench.py at full size:
-# ozaki_gemm with s = 8 reads 167.53 GB and writes 2.16 GB; crt_gemm with q = 15 reads
+# ozaki_gemm with s = 8 reads 83.69 GB and writes 2.15 GB; crt_gemm with q = 15 reads
 # 48.43 GB and writes 4.03 GB.
-OZAKI_GEMM_TRAFFIC_BYTES = 169.69e9
+OZAKI_GEMM_TRAFFIC_BYTES = 85.84e9
 CRT_GEMM_TRAFFIC_BYTES = 52.46e9
 
 

@@ -68,6 +68,7 @@ struct GemmParams {
     double *partial;          // split-K: slice s's scaled result goes to partial + s * partial_stride
     int partial_ld;           // even
     size_t partial_stride;
+    unsigned int *sync;       // this launch's arrival counter (zeroed before the launch), or nullptr
 };
 
 // ---------------------------------------------------------------- shared numerics
@@ -459,6 +460,19 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm(const __grid_constant__
             for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
                 int m0, n0, kb_begin, kb_end;
                 item_of(p, w, m0, n0, kb_begin, kb_end);
+                // Soft lockstep: the CTAs that share a digit slab read it from L2 only while they
+                // stay within a few microseconds of each other, so every producer waits at each
+                // new item until all CTAs have started theirs -- or 20 us, then goes on anyway.
+                // Nothing depends on it for correctness, so it cannot deadlock.
+                if (p.sync) {
+                    atomicAdd(p.sync, 1u);
+                    const unsigned int target = (unsigned int)min((long long)(w / gridDim.x + 1) * gridDim.x,
+                                                                  (long long)items);
+                    const unsigned long long t0 = global_ns();
+                    while (*reinterpret_cast<volatile unsigned int *>(p.sync) < target &&
+                           global_ns() - t0 < 20000ull)
+                        __nanosleep(64);
+                }
                 const uint8_t *ga = p.da + (size_t)(m0 / TILE) * p.kblocks * slab;
                 const uint8_t *gb = p.db + (size_t)(n0 / TILE) * p.kblocks * slab;
                 for (int si = 0; si < p.num_sets && ok; ++si) {
@@ -757,8 +771,26 @@ static size_t ozaki_partial_bytes(int m, int n, int k, int ksplit)
     return align256((size_t)slices * (size_t)m * (size_t)((n + 1) & ~1) * sizeof(double));
 }
 
+// Arrival counters of the products launches' soft lockstep: two per device (one per stream of
+// the host-buffer schedule), library-owned because the workspace of mgx_ozaki_multiply is const.
+// Launches that run at the same time on other streams share them, which only weakens the
+// lockstep (a wait ends after 20 us).
+static __device__ unsigned int g_oz_sync[2];
+
+static unsigned int *oz_sync_ptr(int slot)
+{
+    static std::mutex mu;
+    static void *ptr[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!ptr[dev] && cudaGetSymbolAddress(&ptr[dev], g_oz_sync) != cudaSuccess) ptr[dev] = nullptr;
+    return ptr[dev] ? static_cast<unsigned int *>(ptr[dev]) + (slot & 1) : nullptr;
+}
+
 static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta_one, int s, const unsigned char *ws,
-                               const WsLayout &L, cudaStream_t stream, int ksplit = 1, double *partial = nullptr)
+                               const WsLayout &L, cudaStream_t stream, int ksplit = 1, double *partial = nullptr,
+                               int slot = 0)
 {
     oz::GemmParams p;
     memset(&p, 0, sizeof p);
@@ -803,6 +835,8 @@ static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta
         return MGX_E_WORKSPACE;
     }
     p.status = mgx_device_status_ptr();
+    p.sync = oz_sync_ptr(slot);
+    if (p.sync) MGX_HOST_CHECK(cudaMemsetAsync(p.sync, 0, sizeof(unsigned int), stream));
     const int smem = p.stages * p.stage_bytes + 1024 + 256;
     const int total = ((m + oz::TILE - 1) / oz::TILE) * ((n + oz::TILE - 1) / oz::TILE) * slices;
     const int sms = mgx_sm_count();
@@ -1141,7 +1175,7 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
         double *Cb = dC + (size_t)r0 * n + c0;
         if (ozaki) {
             const WsLayout S = ws_sub(L, r0, c0, splits);
-            rc = ozaki_multiply_impl(Cb, r1 - r0, c1 - c0, k, n, 0, splits, ws, S, cs);
+            rc = ozaki_multiply_impl(Cb, r1 - r0, c1 - c0, k, n, 0, splits, ws, S, cs, 1, nullptr, blk & 1);
         } else if (crt) {
             rc = mgx_crt_host_block(Cb, n, r0, c0, r1 - r0, c1 - c0, m, n, k, splits, ws, cs, blk & 1);
         } else {
