@@ -234,7 +234,9 @@ MGX_API int mgx_ozaki_choose_splits(int k, double exp_range, double target);
  * columns [col_cuts[j], col_cuts[j+1]) of C, and C = 0 followed by C_ij += A_i[:, k0:k0+kc]
  * B_j[k0:k0+kc, :] for every panel of width panel_k.  The plan runs all (block, tile, panel)
  * work in ONE persistent kernel launch (plus the split kernels of the Ozaki form), so a run can
- * be captured in a CUDA graph.  Blocks need not be equal (uneven splits, remainders).
+ * be captured in a CUDA graph.  Blocks need not be equal (uneven splits, remainders).  With the
+ * CRT form (MGX_FORM_CRT) a run is one CRT product of the whole C; its results do not depend on
+ * the block cuts or the panel width.
  * ------------------------------------------------------------------------------------------ */
 
 typedef struct {
@@ -245,7 +247,7 @@ typedef struct {
     const int *col_cuts;       /* likewise for columns */
     int panel_k;               /* panel width BK (MGXBENCH_SUMMA_BK, 2D-block-matrix/mmb.cu:107) */
     int form;                  /* mgx_form_t */
-    int splits;                /* slices of the Ozaki form */
+    int splits;                /* slices of the Ozaki form (2..12), moduli of the CRT form (8..16) */
 } mgx_summa_desc_t;
 
 typedef struct mgx_summa_plan mgx_summa_plan_t;

@@ -7,7 +7,9 @@
 // persistent kernel walks (tile, panel) in order: the FP64 form adds each panel's product into
 // C_ij with one rounding, as the reference does.  The Ozaki form accumulates the panels exactly
 // in int32 and recombines once; because its element values do not depend on how the output is
-// tiled, it covers every block with one uniform 128 x 128 raster of the whole C.
+// tiled, it covers every block with one uniform 128 x 128 raster of the whole C.  The CRT form
+// likewise: its scales belong to whole rows of A and columns of B and its residue sums are exact,
+// so all blocks run as one CRT product of the whole C.
 #include <cstring>
 #include <vector>
 
@@ -18,6 +20,8 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
                         const int4 *tiles, int num_tiles, int panel_kb);
 int mgx_ozaki_run(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb, int ldc,
                   int beta_one, int splits, void *workspace, size_t workspace_bytes, cudaStream_t stream);
+int mgx_crt_run(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb, int ldc,
+                int beta_one, int moduli, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 struct mgx_summa_plan {
     mgx_summa_desc_t desc;
@@ -95,8 +99,9 @@ MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t
 {
     if (!desc || !plan || desc->m <= 0 || desc->n <= 0 || desc->k <= 0 || desc->grid_rows <= 0 ||
         desc->grid_cols <= 0 || desc->grid_rows > desc->m || desc->grid_cols > desc->n || desc->panel_k <= 0 ||
-        (desc->form != MGX_FORM_FP64 && desc->form != MGX_FORM_OZAKI) ||
-        (desc->form == MGX_FORM_OZAKI && (desc->splits < 2 || desc->splits > 12))) {
+        (desc->form != MGX_FORM_FP64 && desc->form != MGX_FORM_OZAKI && desc->form != MGX_FORM_CRT) ||
+        (desc->form == MGX_FORM_OZAKI && (desc->splits < 2 || desc->splits > 12)) ||
+        (desc->form == MGX_FORM_CRT && (desc->splits < 8 || desc->splits > 16))) {
         mgx_set_last_message("mgx_summa_plan_create: invalid descriptor");
         return MGX_E_INVALID;
     }
@@ -123,10 +128,11 @@ MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t
         delete P;
         return MGX_E_CUDA;
     }
-    if (desc->form == MGX_FORM_OZAKI) {
-        P->ws_bytes = mgx_ozaki_workspace_size(desc->m, desc->n, desc->k, desc->splits);
+    if (desc->form == MGX_FORM_OZAKI || desc->form == MGX_FORM_CRT) {
+        P->ws_bytes = desc->form == MGX_FORM_OZAKI ? mgx_ozaki_workspace_size(desc->m, desc->n, desc->k, desc->splits)
+                                                   : mgx_crt_workspace_size(desc->m, desc->n, desc->k, desc->splits);
         if (cudaMalloc(&P->ws, P->ws_bytes) != cudaSuccess) {
-            mgx_set_last_message("mgx_summa_plan_create: Ozaki workspace of %zu bytes", P->ws_bytes);
+            mgx_set_last_message("mgx_summa_plan_create: workspace of %zu bytes", P->ws_bytes);
             cudaFree(P->d_tiles);
             delete P;
             return MGX_E_CUDA;
@@ -147,6 +153,8 @@ MGX_API int mgx_summa_run(mgx_summa_plan_t *P, const double *A, int lda, const d
     cudaStream_t s = (cudaStream_t)stream;
     if (d.form == MGX_FORM_OZAKI)  // element values do not depend on the tiling: one uniform 128 x 128 raster
         return mgx_ozaki_run(A, B, C, d.m, d.n, d.k, lda, ldb, ldc, 0, d.splits, P->ws, P->ws_bytes, s);
+    if (d.form == MGX_FORM_CRT)  // likewise: one CRT product of the whole C
+        return mgx_crt_run(A, B, C, d.m, d.n, d.k, lda, ldb, ldc, 0, d.splits, P->ws, P->ws_bytes, s);
     // C = 0 (2D-block-matrix/mmb.cu:186), then every panel adds into it.
     MGX_HOST_CHECK(cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)d.n * sizeof(double), d.m, s));
     const int bk = d.panel_k < d.k ? d.panel_k : d.k;
