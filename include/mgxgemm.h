@@ -188,6 +188,17 @@ MGX_API int mgx_crt_products(int m, int n, int k, int moduli, void *workspace, s
 MGX_API int mgx_crt_combine(double *C, int m, int n, int k, int ldc, int beta_one, int moduli, void *workspace,
                             size_t workspace_bytes, void *stream);
 
+/* Split-K form of mgx_gemm_ozaki_crt for products with few 256 x 256 output tiles (small m n,
+ * long k): the 32-wide K blocks are cut into `ksplit` slices whose residue products run as
+ * separate work items; the slices' residues are added modulo each p before the CRT rebuild, so
+ * the result is bit-identical to mgx_gemm_ozaki_crt.  Needs k <= mgx_crt_kmax() and
+ * mgx_crt_splitk_workspace_size(m, n, k, moduli, ksplit) bytes of 256-byte aligned workspace
+ * (0 when k is too long).  No counterpart in MGXBench; the autotuner picks ksplit. */
+MGX_API size_t mgx_crt_splitk_workspace_size(int m, int n, int k, int moduli, int ksplit);
+MGX_API int mgx_gemm_ozaki_crt_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda,
+                                      int ldb, int ldc, int beta_one, int moduli, int ksplit, void *workspace,
+                                      size_t workspace_bytes, void *stream);
+
 /* Smallest modulus count whose a-priori normwise error bound meets `target` for reduction
  * length k (8..16). */
 MGX_API int mgx_crt_choose_moduli(int k, double target);

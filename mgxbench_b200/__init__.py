@@ -73,6 +73,8 @@ EXPORTS = [
     ("mgx_ozaki_kmax", _i, [_i]),
     ("mgx_crt_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_ozaki_crt", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_crt_splitk_workspace_size", _sz, [_i, _i, _i, _i, _i]),
+    ("mgx_gemm_ozaki_crt_splitk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_crt_split", _i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_crt_products", _i, [_i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_crt_combine", _i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
@@ -248,12 +250,23 @@ def crt_workspace_size(m, n, k, moduli) -> int:
     return int(lib().mgx_crt_workspace_size(m, n, k, moduli))
 
 
-def gemm_ozaki_crt(A, B, C, moduli: int = 15, beta_one: bool = False, workspace=None, stream=None):
+def crt_splitk_workspace_size(m, n, k, moduli, ksplit) -> int:
+    return int(lib().mgx_crt_splitk_workspace_size(m, n, k, moduli, ksplit))
+
+
+def gemm_ozaki_crt(A, B, C, moduli: int = 15, beta_one: bool = False, workspace=None, stream=None, ksplit: int = 1):
     """C (+)= A B by the CRT form (Ozaki scheme II): one INT8 tensor-core product per modulus,
-    FP64 result rebuilt by the Chinese remainder theorem (mgx_gemm_ozaki_crt)."""
+    FP64 result rebuilt by the Chinese remainder theorem (mgx_gemm_ozaki_crt); ksplit > 1 cuts K
+    into slices computed as separate work items (mgx_gemm_ozaki_crt_splitk, same result)."""
     _check_f64(A, B, C)
     m, k = A.shape
     n = B.shape[1]
+    if ksplit > 1:
+        need = crt_splitk_workspace_size(m, n, k, moduli, ksplit)
+        ws = (workspace or _default_ws).get(need)
+        return _check(lib().mgx_gemm_ozaki_crt_splitk(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
+                                                      int(beta_one), moduli, ksplit, _ptr(ws), ws.numel(),
+                                                      _stream(stream)), "mgx_gemm_ozaki_crt_splitk")
     need = crt_workspace_size(m, n, k, moduli)
     ws = (workspace or _default_ws).get(need)
     return _check(lib().mgx_gemm_ozaki_crt(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),

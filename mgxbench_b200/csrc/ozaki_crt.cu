@@ -402,6 +402,9 @@ struct GemmParams {
     int tiles_m, tiles_n;     // tiles of this block of the product
     int rc_tile_ld;           // tiles per row of the residue planes (the whole product's)
     int kblocks, q;
+    int ksplit;               // K slices per (modulus, tile): 1, or the split-K form's count
+    int kb_split;             // K blocks per slice
+    size_t rc_slice;          // bytes between the residue planes of consecutive K slices
     int *status;
     unsigned int *sync;       // this launch's arrival counter (zeroed before the launch), or nullptr
     uint32_t barrett[MAXQ];
@@ -409,8 +412,10 @@ struct GemmParams {
 
 // Work item w: modulus w / (tiles), then groups of RASTER tile rows sweeping the columns
 // together (the group's rows of A stay in L2 while each column tile of B is read once per group).
-__device__ __forceinline__ void item_of(const GemmParams &p, int w, int &l, int &tm, int &tn)
+__device__ __forceinline__ void item_of(const GemmParams &p, int w, int &l, int &tm, int &tn, int &ks)
 {
+    ks = w % p.ksplit;       // K slice (consecutive items: the same tile's slices)
+    w /= p.ksplit;
     const int per = p.tiles_m * p.tiles_n;
     l = w / per;
     const int t = w - l * per;
@@ -435,7 +440,7 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int items = p.q * p.tiles_m * p.tiles_n;
+    const int items = p.q * p.tiles_m * p.tiles_n * p.ksplit;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -467,8 +472,9 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             for (int s = 0; s < STAGES; ++s) armed[s] = -1;
             bool ok = true;
             for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
-                int l, tm, tn;
-                item_of(p, w, l, tm, tn);
+                int l, tm, tn, ks;
+                item_of(p, w, l, tm, tn, ks);
+                const int kb_begin = ks * p.kb_split, kb_end = min(p.kblocks, kb_begin + p.kb_split);
 #if MGX_CRT_LOCKSTEP
                 // Soft lockstep: CTAs that share an operand tile read it from L2 only while they
                 // stay within a few microseconds of each other, so every producer waits at each
@@ -487,12 +493,12 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
 #endif
                 const uint8_t *ga = p.ra + (size_t)l * p.ra_mod + (size_t)tm * p.kblocks * SLAB;
                 const uint8_t *gb = p.rb + (size_t)l * p.rb_mod + (size_t)tn * p.kblocks * SLAB;
-                for (int kb0 = 0; kb0 < p.kblocks; kb0 += KPACK) {
+                for (int kb0 = kb_begin; kb0 < kb_end; kb0 += KPACK) {
                     if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty)) {
                         ok = false;
                         break;
                     }
-                    const int nkb = min(KPACK, p.kblocks - kb0);
+                    const int nkb = min(KPACK, kb_end - kb0);
                     const uint32_t bytes = (uint32_t)(nkb * SLAB);
                     unsigned char *sa = smem + stage * STAGE_BYTES;
                     mbar_arrive_expect_tx(&full[stage], 2u * bytes);
@@ -522,19 +528,20 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
                 }
                 acc_phase ^= 1u;
                 tc_fence_after();
-                for (int kb0 = 0; kb0 < p.kblocks; kb0 += KPACK) {
+                const int kb_begin = (w % p.ksplit) * p.kb_split, kb_end = min(p.kblocks, kb_begin + p.kb_split);
+                for (int kb0 = kb_begin; kb0 < kb_end; kb0 += KPACK) {
                     if (!mbar_wait_bounded(&full[stage], phase, p.status, kDevTimeoutFull)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const int nkb = min(KPACK, p.kblocks - kb0);
+                    const int nkb = min(KPACK, kb_end - kb0);
                     const uint32_t sa = smem_base + stage * STAGE_BYTES;
                     const uint64_t a0 = sw32_desc(sa), b0 = sw32_desc(sa + KPACK * SLAB);
 #pragma unroll
                     for (int j = 0; j < KPACK; ++j) {
                         if (j < nkb) {
-                            const uint32_t acc = (kb0 + j > 0) ? 1u : 0u;
+                            const uint32_t acc = (kb0 + j > kb_begin) ? 1u : 0u;
                             const uint64_t bj = b0 + (uint64_t)((j * SLAB) >> 4);
                             tc_mma_i8(tmem_base, a0 + (uint64_t)((j * SLAB) >> 4), bj, IDESC_S8_128x256, acc);
                             tc_mma_i8(tmem_base + 256, a0 + (uint64_t)((j * SLAB + SLAB / 2) >> 4), bj,
@@ -566,10 +573,11 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             if (!got) break;
             acc_phase ^= 1u;
             tc_fence_after();
-            int l, tm, tn;
-            item_of(p, w, l, tm, tn);
+            int l, tm, tn, ks;
+            item_of(p, w, l, tm, tn, ks);
             const uint32_t pm = (uint32_t)c_moduli[l], M = p.barrett[l];
-            uint8_t *dst = p.rc + (size_t)l * p.rc_mod + ((size_t)tm * p.rc_tile_ld + tn) * OUT_TILE_BYTES +
+            uint8_t *dst = p.rc + (size_t)ks * p.rc_slice + (size_t)l * p.rc_mod +
+                           ((size_t)tm * p.rc_tile_ld + tn) * OUT_TILE_BYTES +
                            (size_t)((h * 4 + qd) * 32) * 256 + lane * 8;
             const uint32_t tbase = tmem_base + ((uint32_t)(32 * qd) << 16) + h * 256;
             // two 32-column loads in flight per wait, then their reduction and stores
@@ -615,6 +623,8 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
 struct CombineParams {
     const uint8_t *rc;        // the block's first tile of the residue planes
     size_t rc_mod;
+    int ksplit;               // K slices whose residues are added mod p first (1: none)
+    size_t rc_slice;          // bytes between the residue planes of consecutive K slices
     double *C;                // the block's first element of C
     int m, n, ldc, tiles_n, rc_tile_ld, beta_one, vec_store;
     const int *sg, *tu;
@@ -640,13 +650,25 @@ __global__ void __launch_bounds__(256, 3) crt_combine(const __grid_constant__ Co
     for (int j = 0; j < 8; ++j) s1[j] = s2[j] = s3[j] = 0.0;
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
+        uint32_t res[8];
         const uint2 v = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)l * p.rc_mod));
+#pragma unroll
+        for (int j = 0; j < 8; ++j) res[j] = ((j < 4 ? v.x : v.y) >> (8 * (j & 3))) & 255u;
+        if (p.ksplit > 1) {
+            // split-K: the slices' residues (each < p) add modulo p
+            for (int t = 1; t < p.ksplit; ++t) {
+                const uint2 u = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)t * p.rc_slice + (size_t)l * p.rc_mod));
+#pragma unroll
+                for (int j = 0; j < 8; ++j) res[j] += ((j < 4 ? u.x : u.y) >> (8 * (j & 3))) & 255u;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) res[j] = mod_p((int32_t)res[j], (uint32_t)c_moduli[l], p.K.barrett[l]);
+        }
         const double w1 = p.K.w[l][0], w2 = p.K.w[l][1], w3 = p.K.w[l][2];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            // (double) of one byte: 2^52 + b from the bit pattern, minus 2^52 (exact)
-            const double r = __dsub_rn(__hiloint2double(0x43300000, ((j < 4 ? v.x : v.y) >> (8 * (j & 3))) & 255u),
-                                       4503599627370496.0);
+            // (double) of a residue: 2^52 + r from the bit pattern, minus 2^52 (exact)
+            const double r = __dsub_rn(__hiloint2double(0x43300000, res[j]), 4503599627370496.0);
             s1[j] = __fma_rn(w1, r, s1[j]);
             s2[j] = __fma_rn(w2, r, s2[j]);
             s3[j] = __fma_rn(w3, r, s3[j]);
@@ -744,16 +766,23 @@ struct CrtLayout {
     size_t ra, rb, rc, sg, tu, colmax, colsum, sync, total;
     size_t ra_mod, rb_mod, rc_mod;
     int kblocks, tiles_m, tiles_n;
+    int ksplit, kb_split;   // K slices (1: whole K) and K blocks per slice
 };
 
 // Workspace of one K range of at most KMAX: residue slabs of A and B^T (rows rounded up to 256,
 // K to 32), the residue planes of the product, the scale exponents and the column sums.
-CrtLayout crt_layout(int m, int n, int k, int q)
+// With ksplit > 1 (the split-K form, k <= KMAX) the 32-wide K blocks are cut into slices of
+// ceil(kblocks / ksplit) blocks, and the product residues get one set of planes per slice.
+CrtLayout crt_layout(int m, int n, int k, int q, int ksplit = 1)
 {
     CrtLayout L;
     int kc = k < crt::KMAX ? k : crt::KMAX;
     L.kblocks = (kc + 31) / 32;
     if (L.kblocks == 0) L.kblocks = 1;
+    if (ksplit < 1) ksplit = 1;
+    if (ksplit > L.kblocks) ksplit = L.kblocks;
+    L.kb_split = (L.kblocks + ksplit - 1) / ksplit;
+    L.ksplit = (L.kblocks + L.kb_split - 1) / L.kb_split;
     L.tiles_m = (m + crt::TILE - 1) / crt::TILE;
     L.tiles_n = (n + crt::TILE - 1) / crt::TILE;
     L.ra_mod = (size_t)L.tiles_m * L.kblocks * crt::SLAB;
@@ -765,7 +794,7 @@ CrtLayout crt_layout(int m, int n, int k, int q)
     L.rb = off;
     off = align256(off + (size_t)q * L.rb_mod);
     L.rc = off;
-    off = align256(off + (size_t)q * L.rc_mod);
+    off = align256(off + (size_t)q * L.rc_mod * L.ksplit);
     L.sg = off;
     off = align256(off + sizeof(int) * (size_t)m);
     L.tu = off;
@@ -925,10 +954,13 @@ int crt_products_impl(const crt::Consts &K, const CrtLayout &L, const CrtView &v
     p.rc_tile_ld = L.tiles_n;
     p.kblocks = L.kblocks;
     p.q = K.q;
+    p.ksplit = L.ksplit;
+    p.kb_split = L.kb_split;
+    p.rc_slice = (size_t)K.q * L.rc_mod;
     p.status = mgx_device_status_ptr();
     for (int l = 0; l < crt::MAXQ; ++l) p.barrett[l] = K.barrett[l];
     const int smem = crt::STAGES * crt::STAGE_BYTES + 1024 + 256;
-    const long long items = (long long)K.q * v.tiles_m * v.tiles_n;
+    const long long items = (long long)K.q * v.tiles_m * v.tiles_n * L.ksplit;
     if (items <= 0) return MGX_SUCCESS;
     if (items > 0x7fffffffll) {
         mgx_set_last_message("mgx_gemm_ozaki_crt: product too large (%lld work items)", items);
@@ -954,6 +986,8 @@ int crt_combine_impl(double *C, int ldc, int beta_one, const crt::Consts &K, con
     memset(&cp, 0, sizeof cp);
     cp.rc = v.rc;
     cp.rc_mod = L.rc_mod;
+    cp.ksplit = L.ksplit;
+    cp.rc_slice = (size_t)K.q * L.rc_mod;
     cp.C = C;
     cp.m = v.m;
     cp.n = v.n;
@@ -1116,6 +1150,44 @@ int mgx_crt_host_block(double *Cb, int ldc, int r0, int c0, int m, int n, int M,
     const CrtView v = crt_view(L, ws, r0, c0, m, n);
     int rc = crt_products_impl(C, L, v, stream, reinterpret_cast<unsigned int *>(ws + L.sync) + (slot & 1));
     if (rc == MGX_SUCCESS) rc = crt_combine_impl(Cb, ldc, 0, C, L, v, stream);
+    return rc;
+}
+
+extern "C" MGX_API size_t mgx_crt_splitk_workspace_size(int m, int n, int k, int moduli, int ksplit)
+{
+    if (m < 0 || n < 0 || k < 0 || moduli < crt::MINQ || moduli > crt::MAXQ || ksplit < 1 || k > crt::KMAX) return 0;
+    return crt_layout(m, n, k, moduli, ksplit).total;
+}
+
+extern "C" MGX_API int mgx_gemm_ozaki_crt_splitk(const double *A, const double *B, double *C, int m, int n, int k,
+                                                 int lda, int ldb, int ldc, int beta_one, int moduli, int ksplit,
+                                                 void *workspace, size_t workspace_bytes, void *stream)
+{
+    crt::Consts K;
+    if (m < 0 || n < 0 || k < 0 || ksplit < 1 || !crt::make_consts(moduli, K) || (m > 0 && n > 0 && (!C || ldc < n)) ||
+        (m > 0 && n > 0 && k > 0 && (!A || !B || lda < k || ldb < n))) {
+        mgx_set_last_message("mgx_gemm_ozaki_crt_splitk: invalid arguments m=%d n=%d k=%d moduli=%d ksplit=%d", m, n, k,
+                             moduli, ksplit);
+        return MGX_E_INVALID;
+    }
+    if (k > crt::KMAX) {
+        mgx_set_last_message("mgx_gemm_ozaki_crt_splitk: k = %d is above one int32 residue accumulation (%d)", k,
+                             crt::KMAX);
+        return MGX_E_UNSUPPORTED;
+    }
+    if (ksplit == 1 || m == 0 || n == 0 || k == 0)
+        return mgx_crt_run(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, moduli, workspace, workspace_bytes,
+                           (cudaStream_t)stream);
+    const CrtLayout L = crt_layout(m, n, k, moduli, ksplit);
+    if (!workspace || workspace_bytes < L.total || (reinterpret_cast<uintptr_t>(workspace) & 255)) {
+        mgx_set_last_message("mgx_gemm_ozaki_crt_splitk: workspace needs %zu bytes, 256-byte aligned (got %zu)", L.total,
+                             workspace_bytes);
+        return MGX_E_WORKSPACE;
+    }
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = crt_split_impl(A, B, m, n, k, lda, ldb, K, ws, L, st);
+    if (rc == MGX_SUCCESS) rc = crt_multiply_impl(C, m, n, ldc, beta_one ? 1 : 0, K, ws, L, st);
     return rc;
 }
 

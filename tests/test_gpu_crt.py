@@ -144,3 +144,40 @@ def test_crt_host_buffer_path_matches_device_path(mgx, m, n, k, panels):
     mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=15)
     assert np.array_equal(bits(hC.numpy()), bits(host(dC)))
     assert mgx.device_status() == 0
+
+
+@pytest.mark.parametrize("m,n,k,q,ksplit", [
+    (256, 256, 4096, 15, 4), (100, 300, 2000, 14, 3), (513, 130, 1000, 16, 16), (64, 64, 96, 12, 7),
+    (257, 255, 4100, 11, 5), (40, 520, 700, 10, 64)])
+def test_crt_splitk_bit_exact_vs_oracle(mgx, oracle, m, n, k, q, ksplit):
+    """Split-K CRT form: the K slices' residue products are added modulo each p before the CRT
+    rebuild, so the result equals the whole-K form's and the oracle's bit for bit (ksplit is
+    clamped to the K blocks; uneven last slices included)."""
+    import torch
+    rng = np.random.default_rng(m + 3 * n + 5 * k + ksplit)
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    dA, dB = dev(A), dev(B)
+    dC = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dA, dB, dC, moduli=q, ksplit=ksplit)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, q)))
+    whole = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_ozaki_crt(dA, dB, whole, moduli=q)
+    assert torch.equal(whole.view(torch.int64), dC.view(torch.int64))
+    assert mgx.device_status() == 0
+
+
+def test_crt_splitk_beta_one_and_limits(mgx, oracle):
+    import torch
+    rng = np.random.default_rng(8)
+    A, B, C0 = rng_matrix(rng, (130, 3000)), rng_matrix(rng, (3000, 90)), rng_matrix(rng, (130, 90))
+    dC = dev(C0)
+    mgx.gemm_ozaki_crt(dev(A), dev(B), dC, moduli=13, beta_one=True, ksplit=6)
+    assert np.array_equal(bits(host(dC)), bits(oracle.crt_gemm(A, B, 13, C=C0.copy(), beta_one=True)))
+    kmax = mgx.crt_kmax()
+    assert mgx.crt_splitk_workspace_size(8, 8, kmax + 1, 15, 4) == 0
+    assert mgx.crt_splitk_workspace_size(8, 8, kmax, 15, 4) > mgx.crt_workspace_size(8, 8, kmax, 15)
+    X = torch.ones((4, kmax + 32), dtype=torch.float64, device="cuda")
+    with pytest.raises(mgx.MgxError):
+        mgx.gemm_ozaki_crt(X, X.t().contiguous(), torch.empty((4, 4), dtype=torch.float64, device="cuda"),
+                           moduli=15, ksplit=4)
+    assert mgx.device_status() == 0
