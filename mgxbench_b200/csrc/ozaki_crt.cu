@@ -631,8 +631,10 @@ struct CombineParams {
     Consts K;
 };
 
-template <int Q>
-__global__ void __launch_bounds__(256, 3) crt_combine(const __grid_constant__ CombineParams p, long long units)
+// SPLITK: the residue planes of p.ksplit K slices are added modulo p first (a separate
+// instantiation with a larger register budget, so the whole-K kernel keeps its own).
+template <int Q, bool SPLITK>
+__global__ void __launch_bounds__(256, SPLITK ? 2 : 3) crt_combine(const __grid_constant__ CombineParams p, long long units)
 {
     const int lane = threadIdx.x & 31;
     const long long unit = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -654,8 +656,8 @@ __global__ void __launch_bounds__(256, 3) crt_combine(const __grid_constant__ Co
         const uint2 v = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)l * p.rc_mod));
 #pragma unroll
         for (int j = 0; j < 8; ++j) res[j] = ((j < 4 ? v.x : v.y) >> (8 * (j & 3))) & 255u;
-        if (p.ksplit > 1) {
-            // split-K: the slices' residues (each < p) add modulo p
+        if (SPLITK) {
+            // the slices' residues (each < p) add modulo p
             for (int t = 1; t < p.ksplit; ++t) {
                 const uint2 u = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)t * p.rc_slice + (size_t)l * p.rc_mod));
 #pragma unroll
@@ -859,7 +861,10 @@ struct Combine {
     static int run(const crt::CombineParams &cp, long long units, cudaStream_t stream)
     {
         const long long blocks = (units + 7) / 8;
-        crt::crt_combine<Q><<<(unsigned)blocks, 256, 0, stream>>>(cp, units);
+        if (cp.ksplit > 1)
+            crt::crt_combine<Q, true><<<(unsigned)blocks, 256, 0, stream>>>(cp, units);
+        else
+            crt::crt_combine<Q, false><<<(unsigned)blocks, 256, 0, stream>>>(cp, units);
         MGX_HOST_CHECK(cudaGetLastError());
         return MGX_SUCCESS;
     }
