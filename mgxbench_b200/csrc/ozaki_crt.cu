@@ -222,24 +222,60 @@ __global__ void crt_col_scale(const unsigned long long *__restrict__ colmax, con
 // r = y - p rint(y / p), in [-(p-1)/2, (p-1)/2] for odd p, +-128 for 256.  A double
 // 1.5 * 2^52 + z with |z| < 2^51 an integer holds z mod 2^32 in its low word, so
 //   Y = fma(xh, c, xl + 1.5 * 2^52)   (exact)      -> low word y mod 2^32
+//   y = Y - 1.5 * 2^52                (exact)
 //   t = fma(y, 1/p, 1.5 * 2^52)       (one rounding) -> low word rint(y / p): y / p is never
 //       within 2^-9 of a half-integer for odd p, far above the error of the rounded 1/p
 // and r = lo(Y) - p lo(t) in 32-bit arithmetic (r is small, so the wrap-around cancels).
-template <int Q>
-__device__ __forceinline__ void residues(double v, int sg, const Consts &K, uint8_t (&r)[Q])
+// The kernels split 8 values first (split32) and then run each modulus over all 8
+// (residue_word): a modulus's constants are read once per 8 values, and the 8 residue bytes
+// pack into two words with byte permutes.
+constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+
+// 2^e as f1 f2, the factors scale2 multiplies by (f2 = 1 when one factor is enough).
+__device__ __forceinline__ void scale_factors(int e, double &f1, double &f2)
 {
-    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
-    const double x = rint(scale2(v, sg));
-    const double xh = floor(__dmul_rn(x, 2.3283064365386963e-10));  // x * 2^-32
-    const double xl = __fma_rn(-xh, 4294967296.0, x);
-    const double xlr = __dadd_rn(xl, kRound);
-#pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        const double y = __fma_rn(xh, K.c32[l], xl);
-        const double Y = __fma_rn(xh, K.c32[l], xlr);
-        const double t = __fma_rn(y, K.inv_p[l], kRound);
-        r[l] = (uint8_t)((uint32_t)__double2loint(Y) - (uint32_t)__double2loint(t) * (uint32_t)c_moduli[l]);
+    if (e >= -1022 && e <= 1023) {
+        f1 = pow2i(e);
+        f2 = 1.0;
+    } else {
+        const int e1 = e / 2;
+        f1 = pow2i(e1);
+        f2 = pow2i(e - e1);
     }
+}
+
+// x = rint(v 2^sg) as xh 2^32 + xl; returns xh and xl + 1.5 * 2^52.
+__device__ __forceinline__ void split32(double v, double f1, double f2, double &xh, double &xr)
+{
+    const double x = rint(__dmul_rn(__dmul_rn(v, f1), f2));
+    xh = floor(__dmul_rn(x, 2.3283064365386963e-10));  // x * 2^-32
+    xr = __dadd_rn(__fma_rn(-xh, 4294967296.0, x), kRound);
+}
+
+// The residue mod p as the low byte of the returned word (c = 2^32 mod p, ip = 1/p).
+__device__ __forceinline__ uint32_t residue_word(double xh, double xr, double c, double ip, uint32_t p)
+{
+    const double Y = __fma_rn(xh, c, xr);
+    const double t = __fma_rn(__dsub_rn(Y, kRound), ip, kRound);
+    return (uint32_t)__double2loint(Y) - (uint32_t)__double2loint(t) * p;
+}
+
+// Low bytes of a, b, c, d as one word (a in the lowest byte).
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+    return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+// The 8 residue bytes of xh/xr[0..7] for modulus l, element j in byte j.
+template <int Q>
+__device__ __forceinline__ uint2 residues8(const double (&xh)[8], const double (&xr)[8], const Consts &K, int l)
+{
+    const double c = K.c32[l], ip = K.inv_p[l];
+    const uint32_t p = (uint32_t)c_moduli[l];
+    uint32_t w[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) w[j] = residue_word(xh[j], xr[j], c, ip, p);
+    return make_uint2(pack4(w[0], w[1], w[2], w[3]), pack4(w[4], w[5], w[6], w[7]));
 }
 
 // Slab layout: byte (row r, k byte c) of K block kb of 256-row tile t of modulus l sits at
@@ -266,24 +302,21 @@ __global__ void __launch_bounds__(256, 3) crt_split_a(const double *__restrict__
     int s = (row < m) ? sg[row] : 0;
     const bool live = row < m && s != NONFINITE;
     if (!live) s = 0;
-    unsigned long long packed[Q];
-#pragma unroll
-    for (int l = 0; l < Q; ++l) packed[l] = 0;
+    double f1, f2;
+    scale_factors(s, f1, f2);
     const double *arow = A + (size_t)(live ? row : 0) * lda;
+    double xh[8], xr[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int kk = k0 + j;
         double v = (live && kk < k) ? __ldg(arow + kk) : 0.0;
         if (!isfinite(v)) v = 0.0;
-        uint8_t r[Q];
-        residues<Q>(v, s, K, r);
-#pragma unroll
-        for (int l = 0; l < Q; ++l) packed[l] |= (unsigned long long)r[l] << (8 * j);
+        split32(v, f1, f2, xh[j], xr[j]);
     }
     const size_t off = slab_offset(row / TILE, kb, kblocks, row % TILE, kq * 8);
 #pragma unroll
     for (int l = 0; l < Q; ++l)
-        *reinterpret_cast<unsigned long long *>(ra + (size_t)l * mod_stride + off) = packed[l];
+        *reinterpret_cast<uint2 *>(ra + (size_t)l * mod_stride + off) = residues8<Q>(xh, xr, K, l);
 }
 
 // Block: 64 consecutive columns of B x one 32-wide K block.  Warp w takes 32 of the columns
@@ -306,22 +339,19 @@ __global__ void __launch_bounds__(256, 3) crt_split_b(const double *__restrict__
     const bool live = col < n && s != NONFINITE;
     if (!live) s = 0;
     const double *bcol = B + (live ? col : 0);
-    unsigned long long packed[Q];
-#pragma unroll
-    for (int l = 0; l < Q; ++l) packed[l] = 0;
+    double f1, f2;
+    scale_factors(s, f1, f2);
+    double xh[8], xr[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int kk = kb * 32 + kq * 8 + j;
         double v = (live && kk < k) ? __ldg(bcol + (size_t)kk * ldb) : 0.0;
         if (!isfinite(v)) v = 0.0;
-        uint8_t rr[Q];
-        residues<Q>(v, s, K, rr);
-#pragma unroll
-        for (int l = 0; l < Q; ++l) packed[l] |= (unsigned long long)rr[l] << (8 * j);
+        split32(v, f1, f2, xh[j], xr[j]);
     }
     const int soff = rl * 32 + ((kq * 8) ^ (((rl >> 2) & 1) << 4));
 #pragma unroll
-    for (int l = 0; l < Q; ++l) *reinterpret_cast<unsigned long long *>(&st[l][soff]) = packed[l];
+    for (int l = 0; l < Q; ++l) *reinterpret_cast<uint2 *>(&st[l][soff]) = residues8<Q>(xh, xr, K, l);
     __syncthreads();
     const int c0 = blockIdx.x * 64;
     unsigned char *dst = rb + ((size_t)(c0 / TILE) * kblocks + kb) * (size_t)SLAB + (size_t)(c0 % TILE) * 32;
