@@ -34,7 +34,7 @@
 //       warp 1      TMEM owner and MMA issuer: two M=128 N=256 K=32 kind::i8 MMAs per K block
 //                   (rows 0-127 and 128-255), int32 accumulators in all 512 TMEM columns
 //       warps 2-17  epilogue (16 warps, two per accumulator and TMEM lane quarter, 128 columns
-//                   each): tcgen05.ld, exact Barrett reduction mod p_l, one byte per output
+//                   each): tcgen05.ld, exact reduction mod p_l (biased Barrett), one byte per output
 //   crt_combine     CRT recombination of the q residue planes, scaling, (C +) store
 // All waits are bounded (mgx_common.cuh); TMEM is always released before the CTA exits.
 #include <cstdio>
@@ -425,6 +425,17 @@ __device__ __forceinline__ uint32_t mod_p(int32_t g, uint32_t p, uint32_t M)
     return (g >= 0 || r == 0) ? (uint32_t)r : p - (uint32_t)r;
 }
 
+// g mod p in [0, p) for an accumulator of K <= KMAX int8 x int8 products (|g| <= 2^14 K <
+// 2^31 - 2^22): a = g + bias with bias = p floor(2^31 / p) lies in (0, 2^32) and a = g (mod p).
+// Barrett with M = ceil(2^32 / p) gives q = floor(a / p) or one more, so r = a - q p is the
+// residue or the residue minus p (wrapped); the unsigned min of r and r + p is the residue.
+__device__ __forceinline__ uint32_t mod_p_acc(uint32_t g, uint32_t p, uint32_t M, uint32_t bias)
+{
+    const uint32_t a = g + bias;
+    const uint32_t r = a - __umulhi(a, M) * p;
+    return min(r, r + p);
+}
+
 struct GemmParams {
     const uint8_t *ra, *rb;   // residue slabs [modulus][tile][K block][256 x 32 B], at the block's first tile
     uint8_t *rc;              // output residues [modulus][tile row][tile column][64 KiB], at the block's first tile
@@ -438,6 +449,7 @@ struct GemmParams {
     int *status;
     unsigned int *sync;       // this launch's arrival counter (zeroed before the launch), or nullptr
     uint32_t barrett[MAXQ];
+    uint32_t bias[MAXQ];      // p floor(2^31 / p), for mod_p_acc
 };
 
 // Work item w: modulus w / (tiles), then groups of RASTER tile rows sweeping the columns
@@ -605,7 +617,7 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
             tc_fence_after();
             int l, tm, tn, ks;
             item_of(p, w, l, tm, tn, ks);
-            const uint32_t pm = (uint32_t)c_moduli[l], M = p.barrett[l];
+            const uint32_t pm = (uint32_t)c_moduli[l], M = p.barrett[l], bias = p.bias[l];
             uint8_t *dst = p.rc + (size_t)ks * p.rc_slice + (size_t)l * p.rc_mod +
                            ((size_t)tm * p.rc_tile_ld + tn) * OUT_TILE_BYTES +
                            (size_t)((h * 4 + qd) * 32) * 256 + lane * 8;
@@ -622,9 +634,9 @@ __global__ void __launch_bounds__(THREADS, 1) crt_gemm(const __grid_constant__ G
                     uint32_t pk[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
-                        pk[j] = mod_p((int32_t)r[b][4 * j], pm, M) | (mod_p((int32_t)r[b][4 * j + 1], pm, M) << 8) |
-                                (mod_p((int32_t)r[b][4 * j + 2], pm, M) << 16) |
-                                (mod_p((int32_t)r[b][4 * j + 3], pm, M) << 24);
+                        pk[j] = mod_p_acc(r[b][4 * j], pm, M, bias) | (mod_p_acc(r[b][4 * j + 1], pm, M, bias) << 8) |
+                                (mod_p_acc(r[b][4 * j + 2], pm, M, bias) << 16) |
+                                (mod_p_acc(r[b][4 * j + 3], pm, M, bias) << 24);
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
@@ -993,7 +1005,10 @@ int crt_products_impl(const crt::Consts &K, const CrtLayout &L, const CrtView &v
     p.kb_split = L.kb_split;
     p.rc_slice = (size_t)K.q * L.rc_mod;
     p.status = mgx_device_status_ptr();
-    for (int l = 0; l < crt::MAXQ; ++l) p.barrett[l] = K.barrett[l];
+    for (int l = 0; l < crt::MAXQ; ++l) {
+        p.barrett[l] = K.barrett[l];
+        p.bias[l] = (uint32_t)crt::h_moduli[l] * (0x80000000u / (uint32_t)crt::h_moduli[l]);
+    }
     const int smem = crt::STAGES * crt::STAGE_BYTES + 1024 + 256;
     const long long items = (long long)K.q * v.tiles_m * v.tiles_n * L.ksplit;
     if (items <= 0) return MGX_SUCCESS;
