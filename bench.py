@@ -303,8 +303,8 @@ def run_ours(args):
         torch.cuda.empty_cache()
 
     # end to end through the C ABI with pinned host buffers: mgx_gemm_host streams row panels of
-    # A and column panels of B in, computes each block of C once its two panels are on the device
-    # and streams the blocks back while the rest computes
+    # A and column panels of B in; once panel pair t is on the device it computes the new row and
+    # column strips of C (two products) and streams them back while the rest computes
     e2e = None
     if not args.skip_e2e:
         hA = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
@@ -336,8 +336,8 @@ def run_ours(args):
                "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8, "ms_per_step": e2e_ms,
                "bit_identical_to_device_result": same,
                "path": f"mgx_gemm_host via the C ABI: pinned host A, B in, C out; {args.panels} row panels of A x "
-                       f"{args.panels} column panels of B, each block computed once its panels arrive and copied "
-                       f"back while the rest computes"}
+                       f"{args.panels} column panels of B; as each panel pair arrives, the new row and column strips "
+                       f"of C are computed and copied back while the rest computes"}
 
     # roofline of the dominant kernel (crt_gemm, or ozaki_gemm for the slice form): int8 tensor
     # ops per launch / launch time.
@@ -439,7 +439,7 @@ def main():
     ap.add_argument("--splits", type=int, default=0, help="Ozaki slices (0 = chosen for the 1e-15 gate)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--ref-step-seconds", type=float, default=8.0, help="reference arm: seconds per step")
-    ap.add_argument("--panels", type=int, default=8, help="row panels of A and column panels of B in the host-buffer (e2e) path")
+    ap.add_argument("--panels", type=int, default=32, help="row panels of A and column panels of B in the host-buffer (e2e) path")
     ap.add_argument("--skip-native", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

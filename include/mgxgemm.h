@@ -210,8 +210,11 @@ MGX_API int mgx_crt_kmax(void);
  * elements) with form MGX_FORM_FP64, MGX_FORM_OZAKI (`splits` slices) or MGX_FORM_CRT (`splits` =
  * moduli, 8..16).  A is cut into `panels` (1..64) row panels and B into `panels` column panels
  * (multiples of 128; 256 for the CRT form); the panels are copied in the order A_0, B_0,
- * A_1, B_1, ... and every block (i, j) is computed as soon as A_i and B_j are on the device, then
- * copied back while the rest computes, so PCIe copies in both directions overlap the product.
+ * A_1, B_1, ....  Once A_t and B_t are on the device, the blocks (i, j) with max(i, j) = t are
+ * computed as two products (the row strip (t, 0..t) and the column strip (0..t-1, t)) and each
+ * strip is copied back while the rest computes, so PCIe copies in both directions overlap the
+ * product.  At N = 16384, 32 panels keep the last strips short (the end-to-end time is set by
+ * the copies in plus the work the last panels unlock).
  * The result is bit-identical to the device-buffer entry points'.  Device memory (A, B, C and
  * the Ozaki workspace) is taken stream-ordered from the library's pool on the current device
  * and returned before the call's work completes.  Page-locked host memory gives full

@@ -327,7 +327,7 @@ def scratch_trim():
     return _check(lib().mgx_scratch_trim(), "mgx_scratch_trim")
 
 
-def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=8, stream=None):
+def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=32, stream=None):
     """C = A B from host (CPU, ideally pinned) float64 tensors, copies overlapped with compute."""
     import torch
     for t in (hA, hB, hC):

@@ -1127,8 +1127,8 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
 
     cudaStream_t sin = nullptr, sout = nullptr, s1 = nullptr;
     // events: [0] start, [1] s1 done, [2] copies in done, [3] copies out done, then one per A panel,
-    // per B panel, per step (panels prepared) and per block
-    const int nev = 4 + Pm + Pn + T + Pm * Pn;
+    // per B panel, per step (panels prepared) and two per step (its row and column strips)
+    const int nev = 4 + Pm + Pn + T + 2 * T;
     std::vector<cudaEvent_t> ev(nev, nullptr);
     cudaEvent_t *evA = ev.data() + 4, *evB = evA + Pm, *evS = evB + Pn, *evBlk = evS + T;
     int rc = MGX_SUCCESS;
@@ -1167,10 +1167,11 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
             fail(cudaEventRecord(evB[t], sin), "record");
         }
     }
+    // One rectangle of C, rows [r0, r1) x columns [c0, c1) (on the panel grid), computed as one
+    // product on s0 or s1 (alternating) and copied back on sout as soon as it is done.
     int blk = 0;
-    auto run_block = [&](int bi, int bj) {
-        if (rc != MGX_SUCCESS) return;
-        const int r0 = r_at(bi), r1 = r_at(bi + 1), c0 = c_at(bj), c1 = c_at(bj + 1);
+    auto run_rect = [&](int r0, int r1, int c0, int c1) {
+        if (rc != MGX_SUCCESS || r1 <= r0 || c1 <= c0) return;
         cudaStream_t cs = (blk & 1) ? s1 : s0;
         double *Cb = dC + (size_t)r0 * n + c0;
         if (ozaki) {
@@ -1216,11 +1217,11 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
         }
         fail(cudaEventRecord(evS[t], s0), "record");
         fail(cudaStreamWaitEvent(s1, evS[t], 0), "wait");
-        // every block (i, j) with max(i, j) = t
-        if (t < Pm)
-            for (int j = 0; j <= t && j < Pn; ++j) run_block(t, j);
-        if (t < Pn)
-            for (int i = 0; i < t && i < Pm; ++i) run_block(i, t);
+        // every block (i, j) with max(i, j) = t, as two products: the row strip (t, 0..t) and the
+        // column strip (0..t-1, t).  Each element's arithmetic does not depend on the rectangle it
+        // is computed in, so the result is that of the device-buffer entry points.
+        if (t < Pm) run_rect(r_at(t), r_at(t + 1), 0, c_at(t + 1 < Pn ? t + 1 : Pn));
+        if (t < Pn) run_rect(0, r_at(t < Pm ? t : Pm), c_at(t), c_at(t + 1));
     }
     // join the side streams back into the caller's stream, then release the buffers
     if (s1) {
