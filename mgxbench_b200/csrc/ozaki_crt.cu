@@ -291,7 +291,6 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
 }
 
 // The 8 residue bytes of xh/xr[0..7] for modulus l, element j in byte j.
-template <int Q>
 __device__ __forceinline__ uint2 residues8(const double (&xh)[8], const double (&xr)[8], const Consts &K, int l)
 {
     const double c = K.c32[l], ip = K.inv_p[l];
@@ -340,7 +339,7 @@ __global__ void __launch_bounds__(256, 3) crt_split_a(const double *__restrict__
     const size_t off = slab_offset(row / TILE, kb, kblocks, row % TILE, kq * 8);
 #pragma unroll
     for (int l = 0; l < Q; ++l)
-        *reinterpret_cast<uint2 *>(ra + (size_t)l * mod_stride + off) = residues8<Q>(xh, xr, K, l);
+        *reinterpret_cast<uint2 *>(ra + (size_t)l * mod_stride + off) = residues8(xh, xr, K, l);
 }
 
 // Block: 64 consecutive columns of B x one 32-wide K block.  Warp w takes 32 of the columns
@@ -375,7 +374,7 @@ __global__ void __launch_bounds__(256, 3) crt_split_b(const double *__restrict__
     }
     const int soff = rl * 32 + ((kq * 8) ^ (((rl >> 2) & 1) << 4));
 #pragma unroll
-    for (int l = 0; l < Q; ++l) *reinterpret_cast<uint2 *>(&st[l][soff]) = residues8<Q>(xh, xr, K, l);
+    for (int l = 0; l < Q; ++l) *reinterpret_cast<uint2 *>(&st[l][soff]) = residues8(xh, xr, K, l);
     __syncthreads();
     const int c0 = blockIdx.x * 64;
     unsigned char *dst = rb + ((size_t)(c0 / TILE) * kblocks + kb) * (size_t)SLAB + (size_t)(c0 % TILE) * 32;
