@@ -129,10 +129,12 @@ def test_crt_phases_reuse_residues(mgx, oracle):
     assert np.array_equal(bits(first), bits(oracle.crt_gemm(A, B, q)))
 
 
-@pytest.mark.parametrize("m,n,k,panels", [(1000, 700, 900, 3), (512, 512, 256, 1), (300, 1100, 64, 8), (257, 255, 300, 2)])
+@pytest.mark.parametrize("m,n,k,panels", [(1000, 700, 900, 3), (512, 512, 256, 1), (300, 1100, 64, 8), (257, 255, 300, 2),
+                                          (2000, 1500, 300, 32), (1800, 2600, 100, 64)])
 def test_crt_host_buffer_path_matches_device_path(mgx, m, n, k, panels):
-    """mgx_gemm_host with the CRT form (panels of 256 rows/columns prepared as they arrive, blocks
-    computed from them) gives the device path's result bit for bit."""
+    """mgx_gemm_host with the CRT form (panels of 256 rows/columns prepared as they arrive; at
+    each step the new row strip and column strip computed from them, with unequal numbers of
+    row and column panels) gives the device path's result bit for bit."""
     import torch
     rng = np.random.default_rng(m + n + k)
     A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
