@@ -231,8 +231,11 @@ MGX_API int mgx_gemm_host(const double *hA, const double *hB, double *hC, int m,
  * workspace is a fixed device array of MGX_OZAKI_NOALLOC_BYTES that every GPU loading the library
  * holds until exit, so it takes only products whose mgx_ozaki_workspace_size fits (for example
  * m = n = k = 1024 with 8 splits) and returns MGX_E_WORKSPACE otherwise.  The first call on a
- * device looks up the array's device address and should come before any stream capture.  All
- * calls share the array: calls whose work overlaps on the GPU race.  Stream-ordered. */
+ * device looks up the array's device address and should come before any stream capture; the
+ * address is looked up again only when the device's context has changed (after a
+ * cudaDeviceReset), and that call too should come before any capture.  All calls share the
+ * array, and the products' lockstep counters with mgx_gemm_ozaki: calls whose work overlaps on
+ * the GPU race on the array.  Stream-ordered. */
 MGX_API int mgx_gemm_ozaki_noalloc(const double *A, const double *B, double *C, int m, int n, int k, int lda,
                                    int ldb, int ldc, int beta_one, int splits, void *stream);
 
@@ -278,7 +281,13 @@ MGX_API int mgx_summa_plan_create(const mgx_summa_desc_t *desc, mgx_summa_plan_t
 MGX_API int mgx_summa_run(mgx_summa_plan_t *plan, const double *A, int lda, const double *B, int ldb, double *C,
                           int ldc, void *stream);
 
-/* Work tiles (128 x 128, clipped to their blocks), panels and workspace bytes of a plan. */
+/* Work tiles, K steps and workspace bytes of a plan.  FP64 form: the persistent kernel's 128 x 128
+ * tiles clipped to their blocks, and the panels it accumulates in order.  The Ozaki and CRT forms
+ * use no panel list: their integer sums are exact and their scales belong to whole rows and
+ * columns, so neither the block cuts nor the panel order change a bit of C, and the plan runs one
+ * product of all of C.  For them work_tiles is that product's work items (128 x 128 tiles for the
+ * slice form; moduli x 256 x 256 tiles for the CRT form) and panels the number of K chunks of
+ * one exact int32 accumulation (1 unless k > mgx_ozaki_kmax / mgx_crt_kmax). */
 MGX_API int mgx_summa_plan_info(const mgx_summa_plan_t *plan, int *work_tiles, int *panels, size_t *workspace_bytes);
 
 MGX_API int mgx_summa_plan_destroy(mgx_summa_plan_t *plan);

@@ -339,6 +339,20 @@ def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=32, stream=None):
                                       hC.stride(0), form, splits, panels, _stream(stream)), "mgx_gemm_host")
 
 
+# Kernel launches of one product per K chunk of one exact int32 accumulation: the FP64 SUMMA
+# plan's persistent kernel; the slice form's exponent, digit and product kernels; the CRT form's
+# scale, residue, product and recombination kernels.
+_LAUNCHES_PER_CHUNK = {FORM_FP64: 1, FORM_OZAKI: 6, FORM_CRT: 8}
+
+
+def launches_per_product(form: int, k: int, splits: int = 0) -> int:
+    """Kernel launches of one SUMMA-plan product of inner dimension k in the given form."""
+    if form == FORM_FP64:
+        return 1
+    kmax = ozaki_kmax(splits) if form == FORM_OZAKI else crt_kmax()
+    return _LAUNCHES_PER_CHUNK[form] * ((k + kmax - 1) // kmax)
+
+
 def ozaki_kmax(splits: int) -> int:
     return int(lib().mgx_ozaki_kmax(splits))
 

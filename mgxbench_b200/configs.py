@@ -157,11 +157,19 @@ def cfg4(splits=None, model="default"):
         t = _time(g.replay, reps=3)
         e = mgx.error_vs_dd(A, B, C, row_start=M // 2 - 128, row_count=256)
         info = plan.info()
-        out.append({"config": "cfg4", "form": "fp64" if form == mgx.FORM_FP64 else "ozaki", "splits": s or None,
-                    "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}", "panel_k": bk, "panels": info["panels"],
-                    "work_tiles": info["work_tiles"], "tflops": 2 * M * N * K / t / 1e12, "seconds": t,
-                    "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": True,
-                    "persistent_launches_per_product": 1, "splits_from": chooser if s else None})
+        rec = {"config": "cfg4", "form": "fp64" if form == mgx.FORM_FP64 else "ozaki", "splits": s or None,
+               "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}", "panel_k": bk,
+               "tflops": 2 * M * N * K / t / 1e12, "seconds": t,
+               "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": True,
+               "kernel_launches_per_product": mgx.launches_per_product(form, K, s), "splits_from": chooser if s else None}
+        if form == mgx.FORM_FP64:
+            # every block and panel in one persistent kernel
+            rec.update(panels=info["panels"], work_tiles=info["work_tiles"], persistent_launches_per_product=1)
+        else:
+            # the slice form's sums are exact: the plan runs one product of all of C, without the panel list
+            rec.update(panel_list="not used (exact accumulation: one product of all of C)",
+                       k_chunks=info["panels"], product_work_items=info["work_tiles"])
+        out.append(rec)
         del g
         plan.close()
     # the CRT form on the same grid: one whole-K product per block (exact integer sums, so the
@@ -195,7 +203,9 @@ def cfg4(splits=None, model="default"):
     t = _time(g.replay, reps=3)
     e = mgx.error_vs_dd(A, B, C, row_start=M // 2 - 128, row_count=256)
     out.append({"config": "cfg4", "form": "crt", "moduli": q, "m": M, "n": N, "k": K, "grid": f"{pr}x{pc}",
-                "blocks": pr * pc, "launches": "all blocks in one product (SUMMA plan)", "tflops": 2 * M * N * K / t / 1e12,
+                "blocks": pr * pc, "launches": "all blocks in one product (SUMMA plan)",
+                "kernel_launches_per_product": mgx.launches_per_product(mgx.FORM_CRT, K, q),
+                "product_work_items": plan.info()["work_tiles"], "tflops": 2 * M * N * K / t / 1e12,
                 "seconds": t, "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "graph": True,
                 "bit_identical_to_per_block": bool(torch.equal(C.view(torch.int64), per_block.view(torch.int64))),
                 "moduli_from": "crt_choose_moduli"})

@@ -14,7 +14,6 @@ namespace {
 thread_local char g_msg[512] = "";
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-int *g_status_ptr[kMaxDevices];       // device address of mgx_status_word, per device
 int g_sm_count[kMaxDevices];
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 }  // namespace
@@ -42,17 +41,75 @@ static int current_device()
     return dev;
 }
 
+// Id of the context current on this thread (cuCtxGetId), 0 when there is none yet or the driver
+// lacks the call.  A context that cudaDeviceReset ended and the runtime later re-created gets a
+// new id, so an address cached under the old id is known to be stale.
+static unsigned long long current_context_id()
+{
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 4000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(fn);
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of one of this library's __device__ arrays on the current device.  Host code
+// only knows the array's name, a host-side stand-in; the address a kernel needs is taken with
+// cudaGetSymbolAddress in the device's context.  It is cached per device together with the
+// context's id and taken again when the context has changed (after a cudaDeviceReset).  A failed
+// lookup returns nullptr with CUDA's last-error state cleared, so the next launch check does not
+// report it as its own failure; *err (if given) receives the lookup's error.
+void *mgx_symbol_address(const void *symbol, int slot, cudaError_t *err)
+{
+    struct Entry {
+        unsigned long long ctx;
+        void *ptr;
+    };
+    static Entry cache[kMgxSymbolSlots][kMaxDevices];
+    if (err) *err = cudaSuccess;
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices || slot < 0 || slot >= kMgxSymbolSlots) {
+        cudaGetLastError();
+        if (err) *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    Entry &e = cache[slot][dev];
+    unsigned long long ctx = current_context_id();
+    if (e.ptr && ctx != 0 && ctx == e.ctx) return e.ptr;
+    void *p = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&p, symbol);
+    if (rc != cudaSuccess || !p) {
+        cudaGetLastError();
+        if (err) *err = rc != cudaSuccess ? rc : cudaErrorInvalidSymbol;
+        e.ptr = nullptr;
+        return nullptr;
+    }
+    // The lookup itself creates the primary context when none was current yet.
+    if (ctx == 0) ctx = current_context_id();
+    e.ctx = ctx;
+    e.ptr = p;
+    return p;
+}
+
 int *mgx_device_status_ptr()
 {
-    const int dev = current_device();
-    if (dev < 0 || dev >= kMaxDevices) return nullptr;
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_status_ptr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, mgx_status_word) != cudaSuccess) return nullptr;
-        g_status_ptr[dev] = static_cast<int *>(p);
-    }
-    return g_status_ptr[dev];
+    return static_cast<int *>(mgx_symbol_address(reinterpret_cast<const void *>(&mgx_status_word), kMgxSymStatus));
 }
 
 int mgx_sm_count()

@@ -24,6 +24,9 @@
 void mgx_set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line);
 void mgx_set_last_message(const char *fmt, ...);
 int *mgx_device_status_ptr();  // device address of this device's status word (no allocation)
+// The library's file-scope device arrays whose addresses host code looks up.
+enum MgxSymbolSlot : int { kMgxSymStatus = 0, kMgxSymOzSync = 1, kMgxSymOzakiNoalloc = 2, kMgxSymbolSlots = 3 };
+void *mgx_symbol_address(const void *symbol, int slot, cudaError_t *err = nullptr);
 int mgx_sm_count();
 // Stream-ordered scratch from the library's pool on the current device (free with cudaFreeAsync).
 int mgx_scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream);

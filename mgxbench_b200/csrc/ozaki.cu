@@ -779,13 +779,9 @@ static __device__ unsigned int g_oz_sync[2];
 
 static unsigned int *oz_sync_ptr(int slot)
 {
-    static std::mutex mu;
-    static void *ptr[64];
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    std::lock_guard<std::mutex> lk(mu);
-    if (!ptr[dev] && cudaGetSymbolAddress(&ptr[dev], g_oz_sync) != cudaSuccess) ptr[dev] = nullptr;
-    return ptr[dev] ? static_cast<unsigned int *>(ptr[dev]) + (slot & 1) : nullptr;
+    // optional: without it the products run with no lockstep
+    void *p = mgx_symbol_address(reinterpret_cast<const void *>(&g_oz_sync), kMgxSymOzSync);
+    return p ? static_cast<unsigned int *>(p) + (slot & 1) : nullptr;
 }
 
 static int ozaki_multiply_impl(double *C, int m, int n, int k, int ldc, int beta_one, int s, const unsigned char *ws,
@@ -1258,11 +1254,6 @@ extern "C" MGX_API int mgx_gemm_host(const double *hA, const double *hB, double 
 // process exits.  Products whose workspace would not fit are rejected.
 static __device__ __align__(256) unsigned char g_ozaki_noalloc_ws[MGX_OZAKI_NOALLOC_BYTES];
 
-namespace {
-std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[64];
-}  // namespace
-
 extern "C" MGX_API int mgx_gemm_ozaki_noalloc(const double *A, const double *B, double *C, int m, int n, int k,
                                               int lda, int ldb, int ldc, int beta_one, int splits, void *stream)
 {
@@ -1277,28 +1268,14 @@ extern "C" MGX_API int mgx_gemm_ozaki_noalloc(const double *A, const double *B, 
                              need, (unsigned)MGX_OZAKI_NOALLOC_BYTES);
         return MGX_E_WORKSPACE;
     }
-    // The array's name is a host-side stand-in; the kernels need its device address, taken once
-    // per device with that device current (the first call on a device, which should therefore
-    // come before any stream capture).
-    int dev = 0;
-    MGX_HOST_CHECK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) {
-        mgx_set_last_message("mgx_gemm_ozaki_noalloc: device %d out of range", dev);
-        return MGX_E_UNSUPPORTED;
-    }
-    void *ws = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void *p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_ozaki_noalloc_ws);
-            if (e != cudaSuccess || !p) {
-                mgx_set_last_cuda_error(e, "cudaGetSymbolAddress(g_ozaki_noalloc_ws)", __FILE__, __LINE__);
-                return MGX_E_CUDA;
-            }
-            g_noalloc_ptr[dev] = p;
-        }
-        ws = g_noalloc_ptr[dev];
+    // The array's name is a host-side stand-in; the kernels need its device address, taken with
+    // that device current on the first call on each device (which should therefore come before
+    // any stream capture) and again only if the device's context has changed since.
+    cudaError_t e = cudaSuccess;
+    void *ws = mgx_symbol_address(reinterpret_cast<const void *>(&g_ozaki_noalloc_ws), kMgxSymOzakiNoalloc, &e);
+    if (!ws) {
+        mgx_set_last_cuda_error(e, "cudaGetSymbolAddress(g_ozaki_noalloc_ws)", __FILE__, __LINE__);
+        return MGX_E_CUDA;
     }
     // Calls share the array: two calls whose work overlaps on the GPU (different streams, no
     // ordering between them) race on it.  Everything a call reads from the array it first writes

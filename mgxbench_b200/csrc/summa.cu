@@ -174,8 +174,21 @@ MGX_API int mgx_summa_run(mgx_summa_plan_t *P, const double *A, int lda, const d
 MGX_API int mgx_summa_plan_info(const mgx_summa_plan_t *P, int *work_tiles, int *panels, size_t *workspace_bytes)
 {
     if (!P) return MGX_E_INVALID;
-    if (work_tiles) *work_tiles = P->num_tiles;
-    if (panels) *panels = (P->desc.k + P->desc.panel_k - 1) / P->desc.panel_k;
+    const mgx_summa_desc_t &d = P->desc;
+    int tiles = P->num_tiles, steps = (d.k + d.panel_k - 1) / d.panel_k;
+    if (d.form == MGX_FORM_OZAKI) {
+        // one whole product of C: 128 x 128 output tiles, one K chunk per int32 accumulation
+        const int kmax = mgx_ozaki_kmax(d.splits);
+        tiles = ((d.m + 127) / 128) * ((d.n + 127) / 128);
+        steps = kmax > 0 ? (d.k + kmax - 1) / kmax : 1;
+    } else if (d.form == MGX_FORM_CRT) {
+        // one whole product of C: (modulus, 256 x 256 tile) work items, K chunks likewise
+        const int kmax = mgx_crt_kmax();
+        tiles = d.splits * ((d.m + 255) / 256) * ((d.n + 255) / 256);
+        steps = (d.k + kmax - 1) / kmax;
+    }
+    if (work_tiles) *work_tiles = tiles;
+    if (panels) *panels = steps;
     if (workspace_bytes) *workspace_bytes = P->ws_bytes;
     return MGX_SUCCESS;
 }

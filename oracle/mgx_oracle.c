@@ -508,6 +508,7 @@ ORACLE_API int oracle_ozaki_exponents(const double *A, const double *B, int m, i
                                       int32_t *ea, int32_t *eb)
 {
     int nonfinite = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : nonfinite)
     for (int i = 0; i < m; ++i) {
         uint64_t mx = 0;
         for (int kk = 0; kk < k; ++kk) {
@@ -519,6 +520,7 @@ ORACLE_API int oracle_ozaki_exponents(const double *A, const double *B, int m, i
         }
         ea[i] = frexp_exp_bits(mx);
     }
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : nonfinite)
     for (int j = 0; j < n; ++j) {
         uint64_t mx = 0;
         for (int kk = 0; kk < k; ++kk) {
@@ -532,6 +534,8 @@ ORACLE_API int oracle_ozaki_exponents(const double *A, const double *B, int m, i
     }
     return nonfinite;
 }
+
+#define OZ_MAX_SLICES 16
 
 /* Signed radix-2^7 digits of x * 2^(6 - e): |x * 2^(6-e)| < 64, digit_t = rint(r), r <- (r - digit_t) * 128.
  * Every digit lies in [-64, 64]. */
@@ -552,9 +556,11 @@ ORACLE_API void oracle_ozaki_split(const double *A, const double *B, int m, int 
 {
     memset(da, 0, (size_t)s * m * kp);
     memset(db, 0, (size_t)s * n * kp);
+#pragma omp parallel for schedule(dynamic, 4)
     for (int i = 0; i < m; ++i)
         for (int kk = 0; kk < k; ++kk)
             digits_of(A[(size_t)i * lda + kk], ea[i], s, da + (size_t)i * kp + kk, (size_t)m * kp);
+#pragma omp parallel for schedule(dynamic, 4)
     for (int j = 0; j < n; ++j)
         for (int kk = 0; kk < k; ++kk)
             digits_of(B[(size_t)kk * ldb + j], eb[j], s, db + (size_t)j * kp + kk, (size_t)n * kp);
@@ -577,6 +583,7 @@ ORACLE_API int oracle_ozaki_gemm(const double *A, const double *B, double *C, in
                                  int ldb, int ldc, int s, int beta_one, int nthreads)
 {
     nthreads = pick_threads(nthreads);
+    if (s < 1 || s > OZ_MAX_SLICES) return 2;
     int kmax = oracle_ozaki_kmax(s) & ~127;
     if (kmax <= 0) kmax = 128;
     int32_t *ea = (int32_t *)malloc(sizeof(int32_t) * (m > 0 ? m : 1));
@@ -596,10 +603,11 @@ ORACLE_API int oracle_ozaki_gemm(const double *A, const double *B, double *C, in
         int8_t *da = (int8_t *)malloc((size_t)s * m * kp + 1);
         int8_t *db = (int8_t *)malloc((size_t)s * n * kp + 1);
         oracle_ozaki_split(A + k0, B + (size_t)k0 * ldb, m, n, kc, lda, ldb, s, kp, ea, eb, da, db);
-#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+        /* over (i, j) pairs, so that a few rows still use every thread */
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 64) collapse(2)
         for (int i = 0; i < m; ++i) {
-            int64_t *g = (int64_t *)malloc(sizeof(int64_t) * (s + 2));
             for (int j = 0; j < n; ++j) {
+                int64_t g[OZ_MAX_SLICES + 2] = {0};
                 for (int d = 0; d < s + 2; ++d) g[d] = 0;
                 for (int t = 1; t <= s; ++t)
                     for (int u = 1; t + u <= s + 1; ++u) {
@@ -614,7 +622,6 @@ ORACLE_API int oracle_ozaki_gemm(const double *A, const double *B, double *C, in
                 const double r = scale2(h, ea[i] + eb[j] - 12);
                 C[(size_t)i * ldc + j] = C[(size_t)i * ldc + j] + r;
             }
-            free(g);
         }
         free(da);
         free(db);
@@ -808,7 +815,10 @@ ORACLE_API int oracle_crt_scales(const double *A, const double *B, int m, int n,
     crt_consts_t K;
     if (crt_consts(q, &K)) return 2;
     int nonfinite = 0;
+    /* each scale depends on its own row or column only: the loops run in parallel */
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : nonfinite)
     for (int i = 0; i < m; ++i) sigma[i] = crt_sigma(A + (size_t)i * lda, 1, k, K.alpha, &nonfinite);
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : nonfinite)
     for (int j = 0; j < n; ++j) tau[j] = crt_sigma(B + j, (size_t)ldb, k, K.beta, &nonfinite);
     return nonfinite;
 }
@@ -819,6 +829,8 @@ ORACLE_API void oracle_crt_residues(const double *A, const double *B, int m, int
 {
     memset(ra, 0, (size_t)q * m * kp);
     memset(rb, 0, (size_t)q * n * kp);
+    /* every residue depends on its own element only: the loops run in parallel */
+#pragma omp parallel for schedule(dynamic, 4)
     for (int i = 0; i < m; ++i)
         for (int kk = 0; kk < k; ++kk) {
             const double a = A[(size_t)i * lda + kk];
@@ -826,6 +838,7 @@ ORACLE_API void oracle_crt_residues(const double *A, const double *B, int m, int
             const int64_t x = (int64_t)nearbyint(scale2(a, sigma[i]));
             for (int l = 0; l < q; ++l) ra[((size_t)l * m + i) * kp + kk] = crt_residue(x, crt_moduli[l]);
         }
+#pragma omp parallel for schedule(dynamic, 4)
     for (int j = 0; j < n; ++j)
         for (int kk = 0; kk < k; ++kk) {
             const double b = B[(size_t)kk * ldb + j];
@@ -877,10 +890,11 @@ ORACLE_API int oracle_crt_gemm(const double *A, const double *B, double *C, int 
         int8_t *rb = (int8_t *)malloc((size_t)q * n * kp + 1);
         oracle_crt_residues(A + k0, B + (size_t)k0 * ldb, m, n, kc, lda, ldb, q, kp, sg, tu, ra, rb);
         const int add = (k0 > 0) || beta_one;
-#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+        /* over (i, j) pairs, so that a few rows still use every thread */
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 64) collapse(2)
         for (int i = 0; i < m; ++i) {
-            int32_t R[CRT_MAX_MODULI];
             for (int j = 0; j < n; ++j) {
+                int32_t R[CRT_MAX_MODULI];
                 for (int l = 0; l < q; ++l) {
                     const int8_t *pa = ra + ((size_t)l * m + i) * kp;
                     const int8_t *pb = rb + ((size_t)l * n + j) * kp;

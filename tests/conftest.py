@@ -9,6 +9,10 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT))
 
+# MGXBench's own sources, for the tests that run its unmodified scripts or kernels.  They are not
+# part of this repository; tests that need them skip, saying so, where the directory is absent.
+REFERENCE = Path(os.environ.get("MGXBENCH_REFERENCE", "/root/reference"))
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")

@@ -10,11 +10,13 @@ from pathlib import Path
 
 import pytest
 
-from conftest import ROOT
+from conftest import REFERENCE, ROOT
 
 LAUNCHER = ROOT / "mgxbench_b200" / "mgx-onegpu-launch"
 BUILD = ROOT / "build"
-REFERENCE_BENCHMARK = Path("/root/reference/benchmark.py")
+REFERENCE_BENCHMARK = REFERENCE / "benchmark.py"
+RECORDS = ROOT / "tests" / "golden" / "dropin_records.json"
+NO_REFERENCE = f"MGXBench sources not found at {REFERENCE} (set MGXBENCH_REFERENCE)"
 
 
 def _load_launcher():
@@ -56,7 +58,7 @@ def test_launcher_execs_one_process_with_rank_count(tmp_path):
     assert "ranks=2" in out.stdout and "library=SSS" in out.stdout
 
 
-@pytest.mark.skipif(not REFERENCE_BENCHMARK.exists(), reason="MGXBench sources not present")
+@pytest.mark.skipif(not REFERENCE_BENCHMARK.exists(), reason=NO_REFERENCE)
 def test_reference_benchmark_drives_the_launcher(tmp_path):
     """MGXBench's unmodified benchmark.py accepts the one-GPU launcher and our result line."""
     exe = _stub_exe(tmp_path)
@@ -91,3 +93,74 @@ def test_mm2d_argument_errors():
     env = dict(os.environ, MGXBENCH_EMULATED_RANKS="4", MGXBENCH_GRID_ROWS="3")
     r = subprocess.run([str(BUILD / "mm_2d"), "0", "64", "MMM"], capture_output=True, text=True, env=env)
     assert r.returncode == 2 and "invalid process grid" in r.stderr
+
+
+def _replay_exe(build_dir, decomposition, records):
+    """An executable that prints what build/mm_1d or build/mm_2d printed on a GPU for the same
+    size, emulated rank count and library (tests/golden/dropin_records.json), after checking the
+    environment benchmark.py set."""
+    exe = build_dir / ("mm_1d" if decomposition == "1d" else "mm_2d")
+    table = {f"{r['size']}:{r['ranks']}:{r['library']}": r for r in records if r["decomposition"] == decomposition}
+    exe.write_text("#!/usr/bin/env python3\nimport json,os,sys\n"
+                   f"T=json.loads({json.dumps(json.dumps(table))})\n"
+                   "r=T[f\"{sys.argv[2]}:{os.environ['MGXBENCH_EMULATED_RANKS']}:{sys.argv[3]}\"]\n"
+                   "assert os.environ['MGXBENCH_INNER_LOOPS']=='1'\n"
+                   "if r['grid_rows']:\n"
+                   "    assert os.environ['MGXBENCH_GRID_ROWS']==str(r['grid_rows'])\n"
+                   "    assert os.environ['MGXBENCH_GRID_COLS']==str(r['grid_cols'])\n"
+                   "    assert os.environ['MGXBENCH_SUMMA_BK']==str(r['summa_bk'])\n"
+                   "sys.stdout.write(r['stdout']);sys.stderr.write(r['stderr']);sys.exit(r['returncode'])\n")
+    exe.chmod(0o755)
+    return exe
+
+
+@pytest.mark.skipif(not REFERENCE_BENCHMARK.exists(), reason=NO_REFERENCE)
+@pytest.mark.skipif(not RECORDS.exists(), reason="no recorded executable output (tests/golden/make_dropin_records.py)")
+@pytest.mark.parametrize("decomposition", ["1d", "2d"])
+def test_reference_benchmark_accepts_the_executables_output(tmp_path, decomposition):
+    """MGXBench's unmodified benchmark.py, through the one-GPU launcher, accepts what build/mm_1d
+    and build/mm_2d printed on a B200 for the same command lines (recorded by
+    tests/test_gpu_dropin.py / make_dropin_records.py)."""
+    records = json.loads(RECORDS.read_text())
+    mine = [r for r in records if r["decomposition"] == decomposition]
+    assert mine
+    build = tmp_path / "build"
+    build.mkdir()
+    _replay_exe(build, decomposition, records)
+    libs = [r["library"] for r in mine]
+    cmd = [sys.executable, str(REFERENCE_BENCHMARK), "--decomposition", decomposition, "--size", str(mine[0]["size"]),
+           "--ranks", str(mine[0]["ranks"]), "--libraries", *libs, "--warmup", "1", "--repeats", "2",
+           "--launcher", str(LAUNCHER), "--build-dir", str(build), "--output", str(tmp_path / "out")]
+    if decomposition == "2d":
+        cmd += ["--grid-rows", str(mine[0]["grid_rows"]), "--grid-cols", str(mine[0]["grid_cols"]),
+                "--summa-bk", str(mine[0]["summa_bk"])]
+    out = subprocess.run(cmd, capture_output=True, text=True, cwd=str(REFERENCE_BENCHMARK.parent),
+                         env=dict(os.environ, PYTHONDONTWRITEBYTECODE="1"))
+    assert out.returncode == 0, out.stdout + out.stderr
+    doc = json.loads(next((tmp_path / "out").rglob("benchmark.json")).read_text())
+    assert [r["library"] for r in doc["results"]] == libs
+    assert all(r["validated"] and r["ranks"] == mine[0]["ranks"] for r in doc["results"])
+    assert not doc["failures"]
+
+
+@pytest.mark.skipif(not REFERENCE_BENCHMARK.exists(), reason=NO_REFERENCE)
+def test_reference_benchmark_auto_through_the_forwarder(tmp_path):
+    """`benchmark.py --libraries AUTO` imports autotuning.predictive.auto (benchmark.py:83-85).
+    A copy of MGXBench's driver files, made here for the test only, with this library's
+    mgxbench_b200/dropin/autotuning/ in place of its own, reaches the learned cost model's
+    AUTO report (extrapolation model: no GPU needed)."""
+    import shutil
+    tree = tmp_path / "mgxbench"
+    tree.mkdir()
+    shutil.copy(REFERENCE_BENCHMARK, tree / "benchmark.py")
+    shutil.copytree(REFERENCE / "configuration", tree / "configuration")
+    shutil.copytree(ROOT / "mgxbench_b200" / "dropin" / "autotuning", tree / "autotuning")
+    cmd = [sys.executable, str(tree / "benchmark.py"), "--decomposition", "2d", "--size", "8192", "--ranks", "4",
+           "--libraries", "AUTO", "--prediction-model", "extrapolation", "--output", str(tmp_path / "auto")]
+    out = subprocess.run(cmd, capture_output=True, text=True, cwd=str(tree),
+                         env=dict(os.environ, PYTHONDONTWRITEBYTECODE="1", MGXBENCH_B200_ROOT=str(ROOT)))
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "AUTOTUNING REPORT" in out.stdout
+    rep = json.loads((tmp_path / "auto" / "autotuning_prediction.json").read_text())
+    assert rep["status"] == "PREDICTED" and rep["best"]["form"] in ("fp64", "ozaki", "crt")
+    assert rep["decomposition"] == "2d" and rep["ranks"] == 4

@@ -44,6 +44,28 @@ def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(mgx):
     assert L.mgx_device_status(ctypes.byref(code)) == 0 and code.value == 0
 
 
+def test_noalloc_call_leaves_device_memory_unchanged(mgx):
+    """After the first call on the device (which may load the library's kernels), a call takes
+    no device memory: the device's free bytes are the same before and after it."""
+    import torch
+    L = mgx.lib()
+    rng = np.random.default_rng(7)
+    m, n, k, s = 256, 320, 512, 8
+    dA = torch.from_numpy(rng_matrix(rng, (m, k), "wide")).cuda()
+    dB = torch.from_numpy(rng_matrix(rng, (k, n), "wide")).cuda()
+    dC = torch.empty((m, n), dtype=torch.float64, device="cuda")
+    first = torch.empty_like(dC)
+    assert L.mgx_gemm_ozaki_noalloc(_vp(dA), _vp(dB), _vp(first), m, n, k, k, n, n, 0, s, None) == 0
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    rc = L.mgx_gemm_ozaki_noalloc(_vp(dA), _vp(dB), _vp(dC), m, n, k, k, n, n, 0, s, None)
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert rc == 0, L.mgx_last_error_message()
+    assert free_after == free_before
+    assert torch.equal(dC.view(torch.int64), first.view(torch.int64))
+
+
 def test_noalloc_rejects_products_beyond_its_array(mgx):
     L = mgx.lib()
     m = n = k = 4096
