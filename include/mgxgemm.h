@@ -118,6 +118,15 @@ MGX_API int mgx_gemm_fp64_splitk(const double *A, const double *B, double *C, in
                                  int ldb, int ldc, int beta_one, int ksplit, void *workspace,
                                  size_t workspace_bytes, void *stream);
 
+/* mgx_gemm_fp64_splitk with a choice of output tile: tile_m = 128 (128 x 128 tiles, the default
+ * of every other FP64 entry point) or 64 (64 x 128 tiles: twice the work items, for products with
+ * few 128 x 128 tiles on the 148 SMs).  No counterpart in MGXBench; the autotuner's tile
+ * candidates pick it.  Both tiles reduce every element over K in the same order, so the result
+ * does not depend on tile_m.  ksplit and workspace as for mgx_gemm_fp64_splitk. */
+MGX_API int mgx_gemm_fp64_tiled(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                                int ldc, int beta_one, int tile_m, int ksplit, void *workspace,
+                                size_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------------------------------------
  * Ozaki-scheme FP64 GEMM on the INT8 tensor cores (tcgen05, exact int32 TMEM accumulation)
  * ------------------------------------------------------------------------------------------ */

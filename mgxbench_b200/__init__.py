@@ -63,6 +63,7 @@ EXPORTS = [
     ("mgx_gemm_fp64", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp]),
     ("mgx_fp64_splitk_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_fp64_splitk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_gemm_fp64_tiled", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_ozaki", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_splitk_workspace_size", _sz, [_i, _i, _i, _i, _i]),
@@ -185,12 +186,20 @@ def fp64_splitk_workspace_size(m, n, k, ksplit) -> int:
     return int(lib().mgx_fp64_splitk_workspace_size(m, n, k, ksplit))
 
 
-def gemm_fp64(A, B, C, beta_one: bool = False, stream=None, ksplit: int = 1, workspace=None):
+def gemm_fp64(A, B, C, beta_one: bool = False, stream=None, ksplit: int = 1, workspace=None, tile_m: int = 128):
     """C (+)= A B on the FP64 tensor cores; ksplit > 1 cuts K into slices computed by separate
-    CTAs (for products with few output tiles) and needs a workspace (grown on demand)."""
+    CTAs (for products with few output tiles) and needs a workspace (grown on demand); tile_m = 64
+    runs 64 x 128 output tiles instead of 128 x 128 (same result, bit for bit)."""
     _check_f64(A, B, C)
     m, k = A.shape
     n = B.shape[1]
+    if tile_m != 128:
+        need = fp64_splitk_workspace_size(m, n, k, ksplit) if ksplit > 1 else 0
+        ws = (workspace or _default_ws).get(need) if need else None
+        return _check(lib().mgx_gemm_fp64_tiled(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
+                                                int(beta_one), tile_m, ksplit, _ptr(ws) if ws is not None else None,
+                                                ws.numel() if ws is not None else 0, _stream(stream)),
+                      "mgx_gemm_fp64_tiled")
     if ksplit > 1:
         need = fp64_splitk_workspace_size(m, n, k, ksplit)
         ws = (workspace or _default_ws).get(need)
@@ -342,7 +351,7 @@ def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=32, stream=None):
 # Kernel launches of one product per K chunk of one exact int32 accumulation: the FP64 SUMMA
 # plan's persistent kernel; the slice form's exponent, digit and product kernels; the CRT form's
 # scale, residue, product and recombination kernels.
-_LAUNCHES_PER_CHUNK = {FORM_FP64: 1, FORM_OZAKI: 6, FORM_CRT: 8}
+_LAUNCHES_PER_CHUNK = {FORM_FP64: 1, FORM_OZAKI: 6, FORM_CRT: 6}
 
 
 def launches_per_product(form: int, k: int, splits: int = 0) -> int:

@@ -38,7 +38,12 @@ TILE_OZAKI_K4, TILE_OZAKI_K16 = 6, 7
 # CRT form (Ozaki scheme II), 256 x 256 output tiles over the whole K range; its "splits" is the
 # modulus count
 TILE_CRT = 8
-FP64_KSPLIT = {TILE_FP64: 1, TILE_FP64_K2: 2, TILE_FP64_K4: 4, TILE_FP64_K8: 8, TILE_FP64_K16: 16}
+# native FP64 kernel, 64 x 128 output tiles (twice the work items of the 128 x 128 tile), over the
+# whole K range or cut into 2 / 4 / 8 slices
+TILE_FP64_T64, TILE_FP64_T64_K2, TILE_FP64_T64_K4, TILE_FP64_T64_K8 = 9, 10, 11, 12
+FP64_KSPLIT = {TILE_FP64: 1, TILE_FP64_K2: 2, TILE_FP64_K4: 4, TILE_FP64_K8: 8, TILE_FP64_K16: 16,
+               TILE_FP64_T64: 1, TILE_FP64_T64_K2: 2, TILE_FP64_T64_K4: 4, TILE_FP64_T64_K8: 8}
+FP64_TILE_M = {TILE_FP64_T64: 64, TILE_FP64_T64_K2: 64, TILE_FP64_T64_K4: 64, TILE_FP64_T64_K8: 64}
 OZAKI_KSPLIT = {TILE_OZAKI_128: 1, TILE_OZAKI_K4: 4, TILE_OZAKI_K16: 16}
 SPLITS = tuple(range(3, 10))
 CRT_MODULI = (9, 11, 12, 13, 14, 15, 16)
@@ -72,8 +77,13 @@ class Candidate:
         return FP64_KSPLIT.get(self.tile) or OZAKI_KSPLIT.get(self.tile, 1)
 
     @property
+    def tile_m(self) -> int:
+        """Output tile height of an FP64 candidate (64 or 128)."""
+        return FP64_TILE_M.get(self.tile, 128)
+
+    @property
     def name(self) -> str:
-        base = "fp64" if self.is_fp64 else f"{self.form}{self.splits}"
+        base = ("fp64" if self.tile_m == 128 else "fp64t64") if self.is_fp64 else f"{self.form}{self.splits}"
         return base if self.ksplit == 1 else f"{base}k{self.ksplit}"
 
 
@@ -98,7 +108,8 @@ def splitk_applies(m, n, k, ksplit, splits=0):
 
 def candidates(m=None, n=None, k=None):
     """Every configuration, or those that apply to an m x n x k product."""
-    out = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16)]
+    out = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16,
+                                     TILE_FP64_T64, TILE_FP64_T64_K2, TILE_FP64_T64_K4, TILE_FP64_T64_K8)]
     out += [Candidate(t, s) for t in (TILE_OZAKI_128, TILE_OZAKI_K4, TILE_OZAKI_K16) for s in SPLITS]
     out += [Candidate(TILE_CRT, q) for q in CRT_MODULI]
     if m is not None:
@@ -131,7 +142,7 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
     for c in cands:
         def run():
             if c.is_fp64:
-                mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws)
+                mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws, tile_m=c.tile_m)
             elif c.is_crt:
                 mgx.gemm_ozaki_crt(A, B, C, moduli=c.splits, workspace=ws)
             else:

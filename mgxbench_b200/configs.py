@@ -47,25 +47,38 @@ def _mat(r, c, kind, seed, e_range=0):
 
 
 def cfg1():
-    """The drop-in call (mgx_ab_multiply, whole K per tile), then the FP64 tile shape the learned
-    cost model picks for this product (its K slices; 64 output tiles leave most SMs idle)."""
+    """The drop-in call (mgx_ab_multiply: 128 x 128 tiles, whole K), then every FP64 tile shape and
+    K-slice count measured (64 output tiles of 128 x 128 leave most of the 148 SMs idle), and the
+    one the learned cost model picks."""
     n = 1024
     A, B, C = _mat(n, n, 1, 11), _mat(n, n, 1, 12), torch.empty((n, n), dtype=torch.float64, device="cuda")
+    peak = max(mgx.peak_fp64(k, 20000) for k in (3, 4))
     t = _time(lambda: mgx.ab_multiply(A, B, C), reps=20)
     e = mgx.error_vs_dd(A, B, C)
-    out = [{"config": "cfg1", "form": "fp64", "n": n, "ksplit": 1, "tflops": 2 * n ** 3 / t / 1e12, "seconds": t,
+    out = [{"config": "cfg1", "form": "fp64", "n": n, "tile": "128x128", "ksplit": 1, "tflops": 2 * n ** 3 / t / 1e12,
+            "seconds": t, "fp64_peak_tflops": peak, "frac_of_fp64_peak": 2 * n ** 3 / t / 1e12 / peak,
             "normwise_err": e["normwise"], "max_rel_err": e["max_rel"], "rows_checked": e["rows_checked"]}]
     from mgxbench_b200 import autotune as at
     from mgxbench_b200 import predictive as pr_mod
+    fp64 = [c for c in at.candidates(n, n, n) if c.is_fp64]
+    ws = mgx.OzakiWorkspace()
+    measured = {}
+    for c in fp64:
+        measured[c] = _time(lambda: mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws, tile_m=c.tile_m), reps=20)
+    best = min(measured, key=measured.get)
+    out.append({"config": "cfg1", "form": "fp64", "n": n, "measured": {c.name: 2 * n ** 3 / v / 1e12
+                                                                      for c, v in measured.items()},
+                "best": best.name, "best_tflops": 2 * n ** 3 / measured[best] / 1e12,
+                "best_frac_of_fp64_peak": 2 * n ** 3 / measured[best] / 1e12 / peak})
     if pr_mod.DEFAULT_MODEL.is_file():
         model = at.MlpModel.load(pr_mod.DEFAULT_MODEL)
-        fp64 = [c for c in at.candidates(n, n, n) if c.is_fp64]
-        c = at.choose(model, n, n, n, 0, 1.0, fp64)  # the form is fixed; the model picks the K slices
-        ws = mgx.OzakiWorkspace()
-        t2 = _time(lambda: mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws), reps=20)
+        c = at.choose(model, n, n, n, 0, 1.0, fp64)  # the form is fixed; the model picks tile and K slices
+        t2 = _time(lambda: mgx.gemm_fp64(A, B, C, ksplit=c.ksplit, workspace=ws, tile_m=c.tile_m), reps=20)
         e2 = mgx.error_vs_dd(A, B, C)
-        out.append({"config": "cfg1", "form": "fp64", "n": n, "ksplit": c.ksplit, "ksplit_from": "learned cost model",
-                    "tflops": 2 * n ** 3 / t2 / 1e12, "seconds": t2, "normwise_err": e2["normwise"],
+        tf2 = 2 * n ** 3 / t2 / 1e12
+        out.append({"config": "cfg1", "form": "fp64", "n": n, "tile": f"{c.tile_m}x128", "ksplit": c.ksplit,
+                    "choice_from": "learned cost model", "tflops": tf2, "seconds": t2, "frac_of_fp64_peak": tf2 / peak,
+                    "regret_vs_best_measured": t2 / measured[best] - 1, "normwise_err": e2["normwise"],
                     "max_rel_err": e2["max_rel"], "rows_checked": e2["rows_checked"]})
     return out
 

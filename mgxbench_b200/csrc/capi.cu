@@ -240,7 +240,7 @@ int mgx_encode_tmap_3d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_byt
 size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit);
 int mgx_launch_dgemm_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
                             int ldc, int beta_one, int ksplit, void *partial, size_t partial_bytes,
-                            cudaStream_t stream);
+                            cudaStream_t stream, int tile_m = 128);
 
 int mgx_launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                      int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic);
@@ -353,6 +353,21 @@ MGX_API int mgx_gemm_fp64_splitk(const double *A, const double *B, double *C, in
     }
     return mgx_launch_dgemm_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, ksplit, workspace,
                                    workspace_bytes, (cudaStream_t)stream);
+}
+
+MGX_API int mgx_gemm_fp64_tiled(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                                int ldc, int beta_one, int tile_m, int ksplit, void *workspace,
+                                size_t workspace_bytes, void *stream)
+{
+    if (!dims_ok(m, n, k, lda, ldb, ldc) || ksplit < 1 || (tile_m != 64 && tile_m != 128) ||
+        (m > 0 && n > 0 && (!C || (k > 0 && (!A || !B))))) {
+        mgx_set_last_message("mgx_gemm_fp64_tiled: invalid arguments m=%d n=%d k=%d lda=%d ldb=%d ldc=%d tile_m=%d "
+                             "(64 or 128) ksplit=%d",
+                             m, n, k, lda, ldb, ldc, tile_m, ksplit);
+        return MGX_E_INVALID;
+    }
+    return mgx_launch_dgemm_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, ksplit, workspace,
+                                   workspace_bytes, (cudaStream_t)stream, tile_m);
 }
 
 MGX_API int mgx_ab_multiply(double *a, double *b, double *c, int m, int n, int k, int lda, int ldb, int ldc, int w)

@@ -23,8 +23,11 @@
 namespace mgx {
 namespace fp64 {
 
+// Output tiles are BM x 128 with BM = 128 (the default) or 64 (the small-product tile: twice the
+// work items, so a product with few 128 x 128 tiles fills more of the 148 SMs); both reduce each
+// element over K in the same order, so their results are bit-identical.
 constexpr int BM = 128, BN = 128, BK = 32;
-constexpr int STAGES = 3;
+constexpr int BM_SMALL = 64;
 constexpr int CWARPS = 8;
 constexpr int PRODUCER_WARPS = 4;                         // one warpgroup; its warp 0 issues the loads
 constexpr int THREADS = (CWARPS + PRODUCER_WARPS) * 32;   // 384 = 3 warpgroups
@@ -35,13 +38,21 @@ constexpr int THREADS = (CWARPS + PRODUCER_WARPS) * 32;   // 384 = 3 warpgroups
 constexpr int LAUNCH_REGS = 168, PRODUCER_REGS = 40, CONSUMER_REGS = 232;
 static_assert(PRODUCER_WARPS * 32 * PRODUCER_REGS + CWARPS * 32 * CONSUMER_REGS == THREADS * LAUNCH_REGS,
               "register split must equal the launch budget");
-constexpr int A_BOX_BYTES = 128 * 128;       // 128 rows x 16 doubles
 constexpr int B_BOX_BYTES = BK * 128;        // 32 rows x 16 doubles
-constexpr int A_STAGE_BYTES = 2 * A_BOX_BYTES;
 constexpr int B_STAGE_BYTES = 8 * B_BOX_BYTES;
-constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;  // 64 KiB
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr int GROUP_M = 8;
+
+// Shared-memory geometry of a BM-row tile: A as two boxes of BM rows x 16 doubles, B as eight
+// boxes of 32 rows x 16 doubles; 3 stages of 64 KiB for BM = 128, 4 of 48 KiB for BM = 64.
+template <int TBM>
+struct Geo {
+    static constexpr int A_BOX_BYTES = TBM * 128;
+    static constexpr int A_STAGE_BYTES = 2 * A_BOX_BYTES;
+    static constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
+    static constexpr int STAGES = TBM == 128 ? 3 : 4;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int MT = TBM / 32;          // 16-row MMA tiles per consumer warp (2 x 4 warp grid)
+    static constexpr int GROUP_M = 1024 / TBM;   // raster groups of 1024 rows
+};
 
 struct Params {
     const double *A;  // generic loader only
@@ -66,12 +77,14 @@ struct Params {
     size_t partial_stride;
 };
 
+template <int TBM>
 __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn);
 
 // Tile geometry.  n0 is where the tile's columns start in B and C; it is always even, because it
 // is the x coordinate of B's TMA boxes and TMA needs x * 8 bytes to be a multiple of 16.  A work
 // item may begin at an odd column n_lo (uneven SUMMA blocks): its tile then starts one column
 // earlier and the columns below n_lo, which belong to the neighbouring block, are not stored.
+template <int TBM>
 __device__ __forceinline__ void tile_bounds(const Params &p, int tile, int tiles_m, int tiles_n, int &m0, int &n0,
                                             int &m_end, int &n_end, int &n_lo)
 {
@@ -84,8 +97,8 @@ __device__ __forceinline__ void tile_bounds(const Params &p, int tile, int tiles
         n_end = t.w;
     } else {
         int tm, tn;
-        tile_coords(tile, tiles_m, tiles_n, tm, tn);
-        m0 = tm * BM;
+        tile_coords<TBM>(tile, tiles_m, tiles_n, tm, tn);
+        m0 = tm * TBM;
         n0 = tn * BN;
         n_lo = n0;
         m_end = p.m;
@@ -93,8 +106,10 @@ __device__ __forceinline__ void tile_bounds(const Params &p, int tile, int tiles
     }
 }
 
+template <int TBM>
 __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn)
 {
+    constexpr int GROUP_M = Geo<TBM>::GROUP_M;
     const int per_group = GROUP_M * tiles_n;
     const int group = tile / per_group;
     const int first_m = group * GROUP_M;
@@ -105,13 +120,14 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 }
 
 // Work item w: its output tile and the K blocks [kb_begin, kb_end) it reduces over.
+template <int TBM>
 __device__ __forceinline__ void item_bounds(const Params &p, int w, int tiles_m, int tiles_n, int kblocks, int &m0,
                                             int &n0, int &m_end, int &n_end, int &n_lo, int &kb_begin, int &kb_end,
                                             int &slice)
 {
     const int tile = p.ksplit > 1 ? w / p.ksplit : w;
     slice = p.ksplit > 1 ? w % p.ksplit : 0;
-    tile_bounds(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
+    tile_bounds<TBM>(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
     kb_begin = slice * p.kb_split;
     kb_end = min(kblocks, kb_begin + p.kb_split);
 }
@@ -122,10 +138,13 @@ __device__ __forceinline__ uint32_t sw128(int row, int col16)
     return row * 128 + ((((col16 >> 1) ^ (row & 7)) & 7) << 4) + ((col16 & 1) << 3);
 }
 
-template <bool USE_TMA, bool PANELS>
+template <int TBM, bool USE_TMA, bool PANELS>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
 {
+    using G = Geo<TBM>;
+    constexpr int STAGES = G::STAGES, STAGE_BYTES = G::STAGE_BYTES, A_STAGE_BYTES = G::A_STAGE_BYTES;
+    constexpr int A_BOX_BYTES = G::A_BOX_BYTES, MT = G::MT;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                             ~uintptr_t(1023));
@@ -148,7 +167,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     __syncthreads();
 
-    const int tiles_m = (p.m + BM - 1) / BM;
+    const int tiles_m = (p.m + TBM - 1) / TBM;
     const int tiles_n = (p.n + BN - 1) / BN;
     const int tiles = p.tiles ? p.num_tiles : tiles_m * tiles_n;
     const int kblocks = (p.k_len + BK - 1) / BK;
@@ -165,7 +184,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         bool ok = true;
         for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
             int m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
-            item_bounds(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
+            item_bounds<TBM>(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
             for (int kb = kb_begin; kb < kb_end; ++kb) {
                 bool got = true;
                 if (lane == 0) got = mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty);
@@ -187,8 +206,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                         for (int j = 0; j < 8; ++j) tma_load_2d(sB + j * B_BOX_BYTES, &tmB, n0 + 16 * j, k0, &full[stage]);
                     }
                 } else {
-                    // A tile: 128 rows x 32 columns, one row per warp iteration (coalesced)
-                    for (int r = 0; r < BM; ++r) {
+                    // A tile: TBM rows x 32 columns, one row per warp iteration (coalesced)
+                    for (int r = 0; r < TBM; ++r) {
                         const int row = m0 + r;
                         const int kk = k0 + lane;
                         const int acol = p.a_x0 + kk;
@@ -236,13 +255,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t smem_base = smem_u32(smem);
 
     // Per-lane parts of the fragment addresses (see the header comment for the permutation).
-    uint32_t a_row_off[4][2];
-    for (int mt = 0; mt < 4; ++mt)
-        for (int h = 0; h < 2; ++h) a_row_off[mt][h] = (uint32_t)((wm * 64 + mt * 16 + h * 8 + g) * 128 + ((t & 1) << 3));
+    uint32_t a_row_off[MT][2];
+    for (int mt = 0; mt < MT; ++mt)
+        for (int h = 0; h < 2; ++h)
+            a_row_off[mt][h] = (uint32_t)((wm * (TBM / 2) + mt * 16 + h * 8 + g) * 128 + ((t & 1) << 3));
 
     // dst (+)= acc for this lane's fragments, masked to the tile's bounds (dst = C, or a split-K
     // slice of the partial products).
-    auto store_acc = [&](double (&acc)[4][4][4], int m0, int n0, int m_end, int n_end, int n_lo, int beta_one,
+    auto store_acc = [&](double (&acc)[MT][4][4], int m0, int n0, int m_end, int n_end, int n_lo, int beta_one,
                          double *dst_base, int ld, int vec_store) {
         if (PANELS) {
             // SUMMA panels: C += acc as fire-and-forget L2 reductions, so the consumers go on with
@@ -250,10 +270,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             // the load-add-store it replaces; one thread owns each element, and its adds to one
             // address stay in program order, so the panel order of the sums is kept.
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt) {
+            for (int mt = 0; mt < MT; ++mt) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
+                    const int row = m0 + wm * (TBM / 2) + mt * 16 + h * 8 + g;
                     if (row >= m_end) continue;
                     double *crow = dst_base + (size_t)row * ld;
 #pragma unroll
@@ -272,10 +292,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         } else {
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt) {
+            for (int mt = 0; mt < MT; ++mt) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int row = m0 + wm * 64 + mt * 16 + h * 8 + g;
+                    const int row = m0 + wm * (TBM / 2) + mt * 16 + h * 8 + g;
                     if (row >= m_end) continue;
                     double *crow = dst_base + (size_t)row * ld;
 #pragma unroll
@@ -303,11 +323,11 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     for (int w = blockIdx.x; w < items; w += gridDim.x) {
         int m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
-        item_bounds(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
+        item_bounds<TBM>(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
 
-        double acc[4][4][4];
+        double acc[MT][4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < MT; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -346,7 +366,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint32_t c0 = (uint32_t)((((kb8 & 1) * 4 + (t >> 1) * 2) ^ g) << 4);
                 const uint32_t c1 = (uint32_t)((((kb8 & 1) * 4 + (t >> 1) * 2 + 1) ^ g) << 4);
 #pragma unroll
-                for (int mt = 0; mt < 4; ++mt) {
+                for (int mt = 0; mt < MT; ++mt) {
                     double af[4];
                     af[0] = lds_f64(abase + c0 + a_row_off[mt][0]);
                     af[1] = lds_f64(abase + c0 + a_row_off[mt][1]);
@@ -366,7 +386,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 // end of a SUMMA panel: C_ij += panel product, one rounding, as the reference
                 store_acc(acc, m0, n0, m_end, n_end, n_lo, 1, p.C, p.ldc, p.vec_store);
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < MT; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -445,9 +465,9 @@ __global__ void pack_kernel(const double *__restrict__ src, int src_rows, int ld
 
 using namespace mgx;
 
-static int tiles_list_or(const int4 *tiles, int num_tiles, int m, int n)
+static int tiles_list_or(const int4 *tiles, int num_tiles, int m, int n, int bm)
 {
-    return tiles ? num_tiles : ((m + fp64::BM - 1) / fp64::BM) * ((n + fp64::BN - 1) / fp64::BN);
+    return tiles ? num_tiles : ((m + bm - 1) / bm) * ((n + fp64::BN - 1) / fp64::BN);
 }
 
 // Split-K geometry: K blocks per slice and the number of non-empty slices for `ksplit` asked.
@@ -483,7 +503,7 @@ size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit)
 static int launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                         int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
                         const int4 *tiles, int num_tiles, int panel_kb, int ksplit, void *partial,
-                        size_t partial_bytes);
+                        size_t partial_bytes, int bm = fp64::BM);
 
 // Launch C (+)= A[:, a_x0 : a_x0 + k_len] * B[0 : k_len, :] with the library's FP64 kernel.
 // a_x_end: A columns at or beyond it read as zero; b_rows: rows of B that exist.
@@ -500,17 +520,19 @@ int mgx_launch_dgemm_ex(const double *A, const double *B, double *C, int m, int 
 // into C in slice order by a second kernel.
 int mgx_launch_dgemm_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
                             int ldc, int beta_one, int ksplit, void *partial, size_t partial_bytes,
-                            cudaStream_t stream)
+                            cudaStream_t stream, int tile_m)
 {
     return launch_dgemm(A, B, C, m, n, k, 0, k, k, lda, ldb, ldc, beta_one, stream, 0, nullptr, 0, 0, ksplit,
-                        partial, partial_bytes);
+                        partial, partial_bytes, tile_m == fp64::BM_SMALL ? fp64::BM_SMALL : fp64::BM);
 }
 
 static int launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                         int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
                         const int4 *tiles, int num_tiles, int panel_kb, int ksplit, void *partial,
-                        size_t partial_bytes)
+                        size_t partial_bytes, int bm)
 {
+    // SUMMA work lists and panel accumulation are laid out for 128-row tiles
+    if (tiles || panel_kb > 0) bm = fp64::BM;
     if (m <= 0 || n <= 0) return MGX_SUCCESS;
     if (k_len <= 0) {
         if (beta_one) return MGX_SUCCESS;
@@ -580,7 +602,7 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
         } else {
             rc = launch_dgemm(A2 ? A2 : A, B2 ? B2 : B, C, m, n, k_len, A2 ? 0 : a_x0, A2 ? k_len : a_x_end,
                               B2 ? k_len : b_rows, A2 ? lda2 : lda, B2 ? ldb2 : ldb, ldc, beta_one, stream, 0, tiles,
-                              num_tiles, panel_kb, ksplit, partial, partial_bytes);
+                              num_tiles, panel_kb, ksplit, partial, partial_bytes, bm);
         }
         cudaFreeAsync(scratch, stream);
         return rc;
@@ -592,15 +614,15 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
     bool use_tma = false;
     if (tma_ok) {
         const int ea = mgx_encode_tmap_2d(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, (uint64_t)a_x_end, (uint64_t)m,
-                                          (uint64_t)lda * 8, 16, 128, CU_TENSOR_MAP_SWIZZLE_128B);
+                                          (uint64_t)lda * 8, 16, (uint32_t)bm, CU_TENSOR_MAP_SWIZZLE_128B);
         const int eb = mgx_encode_tmap_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, B, (uint64_t)n, (uint64_t)b_rows,
                                           (uint64_t)ldb * 8, 16, fp64::BK, CU_TENSOR_MAP_SWIZZLE_128B);
         use_tma = (ea == MGX_SUCCESS && eb == MGX_SUCCESS);
     }
-    const int total_items = tiles_list_or(tiles, num_tiles, m, n) * slices;
+    const int total_items = tiles_list_or(tiles, num_tiles, m, n, bm) * slices;
     int grid = mgx_sm_count();
     if (grid > total_items) grid = total_items;
-    auto launch = [&](auto kernel) -> int {
+    auto launch = [&](auto kernel, int smem_bytes) -> int {
         cudaFuncAttributes fa;
         MGX_HOST_CHECK(cudaFuncGetAttributes(&fa, kernel));
         if (fa.numRegs != fp64::LAUNCH_REGS) {
@@ -608,15 +630,21 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
                                  fa.numRegs, fp64::LAUNCH_REGS);
             return MGX_E_UNSUPPORTED;
         }
-        MGX_HOST_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, fp64::SMEM_BYTES));
-        kernel<<<grid, fp64::THREADS, fp64::SMEM_BYTES, stream>>>(tmA, tmB, p);
+        MGX_HOST_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
+        kernel<<<grid, fp64::THREADS, smem_bytes, stream>>>(tmA, tmB, p);
         return MGX_SUCCESS;
     };
+    constexpr int S128 = fp64::Geo<fp64::BM>::SMEM_BYTES, S64 = fp64::Geo<fp64::BM_SMALL>::SMEM_BYTES;
     int rc;
-    if (use_tma)
-        rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<true, true>) : launch(fp64::dgemm_kernel<true, false>);
+    if (bm == fp64::BM_SMALL)
+        rc = use_tma ? launch(fp64::dgemm_kernel<fp64::BM_SMALL, true, false>, S64)
+                     : launch(fp64::dgemm_kernel<fp64::BM_SMALL, false, false>, S64);
+    else if (use_tma)
+        rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<fp64::BM, true, true>, S128)
+                          : launch(fp64::dgemm_kernel<fp64::BM, true, false>, S128);
     else
-        rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<false, true>) : launch(fp64::dgemm_kernel<false, false>);
+        rc = panel_kb > 0 ? launch(fp64::dgemm_kernel<fp64::BM, false, true>, S128)
+                          : launch(fp64::dgemm_kernel<fp64::BM, false, false>, S128);
     if (rc != MGX_SUCCESS) return rc;
     MGX_HOST_CHECK(cudaGetLastError());
     if (slices > 1) {

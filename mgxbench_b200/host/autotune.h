@@ -30,6 +30,7 @@ struct AutoChoice {
     int form = -1;        // MGX_FORM_FP64, MGX_FORM_OZAKI or MGX_FORM_CRT
     int splits = 0;
     int ksplit = 1;       // FP64 split-K slices
+    int tile_m = 128;     // FP64 output tile height (64 or 128)
     double predicted_s = 0.0;
     double predicted_err = 0.0;
     std::string model_path;
@@ -80,9 +81,10 @@ inline std::string exe_dir()
 
 inline std::string default_model_path() { return exe_dir() + "/../mgxbench_b200/data/mlp_b200.json"; }
 
-// Tile ids of the candidates (mgxbench_b200.autotune): 0, 2, 3, 4, 5 are the FP64 kernel with
-// the K range cut into 1, 2, 4, 8, 16 slices; 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices;
-// 8 is the CRT form (its "splits" is the modulus count).
+// Tile ids of the candidates (mgxbench_b200.autotune): 0, 2, 3, 4, 5 are the FP64 kernel's
+// 128 x 128 tiles with the K range cut into 1, 2, 4, 8, 16 slices; 9, 10, 11, 12 its 64 x 128
+// tiles with 1, 2, 4, 8 slices; 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices; 8 is the CRT
+// form (its "splits" is the modulus count).
 inline int tile_ksplit(int tile)
 {
     switch (tile) {
@@ -92,10 +94,14 @@ inline int tile_ksplit(int tile)
     case 5: return 16;
     case 6: return 4;
     case 7: return 16;
+    case 10: return 2;
+    case 11: return 4;
+    case 12: return 8;
     default: return 1;
     }
 }
 
+inline int tile_rows(int tile) { return (tile >= 9 && tile <= 12) ? 64 : 128; }
 inline bool tile_is_crt(int tile) { return tile == 8; }
 inline bool tile_is_fp64(int tile) { return tile != 1 && tile != 6 && tile != 7 && !tile_is_crt(tile); }
 
@@ -134,8 +140,10 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
         return -1;
     }
     if (!json_numbers(text, "candidates", &cand) || cand.empty() || cand.size() % 2) {
-        cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0};  // default list: FP64 (1..16 K slices), Ozaki 3..9 splits
-        for (int t : {1, 6, 7})                 // with 1, 4, 16 K slices, CRT 9, 11..16 moduli
+        // default list: FP64 128-row tiles (1..16 K slices) and 64-row tiles (1..8), Ozaki 3..9
+        // splits with 1, 4, 16 K slices, CRT 9, 11..16 moduli
+        cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0, 9, 0, 10, 0, 11, 0, 12, 0};
+        for (int t : {1, 6, 7})
             for (int s = 3; s <= 9; ++s) {
                 cand.push_back(t);
                 cand.push_back(s);
@@ -213,6 +221,7 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
                 : tile_is_fp64((int)cand[2 * pick]) ? MGX_FORM_FP64 : MGX_FORM_OZAKI;
     out->splits = (int)cand[2 * pick + 1];
     out->ksplit = tile_ksplit((int)cand[2 * pick]);
+    out->tile_m = tile_rows((int)cand[2 * pick]);
     out->predicted_s = std::exp(Y[(size_t)pick * 2] * ystd[0] + ymean[0]);
     out->predicted_err = std::pow(10.0, Y[(size_t)pick * 2 + 1] * ystd[1] + ymean[1]);
     out->model_path = path;
@@ -232,8 +241,8 @@ inline double auto_target()
 // ../mgxbench_b200/data/mlp_b200.json beside the executable); the target is
 // MGXBENCH_TARGET_ERR (normwise, default 1e-15).  Exits with `exit_code` if the model is
 // unusable: AUTO without a model is an error, as in MGXBench (autotuning/predictive.py:609-611).
-inline void resolve_auto_form(int *form, int *splits, int *ksplit, std::string *form_name, int m, int n, int k,
-                              double exp_range, int exit_code, bool whole_k_only)
+inline void resolve_auto_form(int *form, int *splits, int *ksplit, int *tile_m, std::string *form_name, int m, int n,
+                              int k, double exp_range, int exit_code, bool whole_k_only)
 {
     if (*form != 2) return;
     const char *env = getenv("MGXBENCH_AUTO_MODEL");
@@ -249,10 +258,11 @@ inline void resolve_auto_form(int *form, int *splits, int *ksplit, std::string *
     *form = c.form == MGX_FORM_OZAKI ? 1 : (c.form == MGX_FORM_CRT ? 3 : 0);
     *splits = c.form == MGX_FORM_FP64 ? 0 : c.splits;
     *ksplit = c.ksplit;
+    *tile_m = c.form == MGX_FORM_FP64 ? c.tile_m : 128;
     *form_name = c.form == MGX_FORM_OZAKI ? "ozaki" : (c.form == MGX_FORM_CRT ? "crt" : "fp64");
     printf("mmb autotune: model=%s m=%d n=%d k=%d exp_range=%g target=%.3e choice=%s splits=%d ksplit=%d "
-           "predicted_s=%.6e predicted_err=%.3e\n",
-           path.c_str(), m, n, k, exp_range, target, form_name->c_str(), *splits, *ksplit, c.predicted_s,
+           "tile_m=%d predicted_s=%.6e predicted_err=%.3e\n",
+           path.c_str(), m, n, k, exp_range, target, form_name->c_str(), *splits, *ksplit, *tile_m, c.predicted_s,
            c.predicted_err);
 }
 

@@ -82,18 +82,20 @@ int main(int argc, char *argv[])
     const bool chunked = (libB == 'S' || libB == 'Y' || libB == 'X');
     int splits = mm::env_int("MGXBENCH_SPLITS", 8);
     int ksplit = mm::env_int("MGXBENCH_KSPLIT", 1);
+    int tile_m = mm::env_int("MGXBENCH_TILE_M", 128) == 64 ? 64 : 128;
     const bool batched = mm::env_int("MGXBENCH_BATCH", 1) != 0;
     const int launches = batched ? 1 : nRanks;
     const int rows_per_launch = batched ? m : mi;
     const bool autotuned = form == mm::kAuto;
     // the choice is made for the product one launch runs (its K chunk when chunked)
-    mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, rows_per_launch, n,
+    mm::resolve_auto_form(&form, &splits, &ksplit, &tile_m, &form_name, rows_per_launch, n,
                           chunked ? std::min(pipeline_k_chunk, k) : k,
                           input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, EXIT_FAILURE, chunked);
     if (chunked) ksplit = 1;
     if (form == mm::kCrt && !autotuned)
         splits = mm::env_int("MGXBENCH_MODULI", mgx_crt_choose_moduli(chunked ? std::min(pipeline_k_chunk, k) : k, 1e-15));
     if (form == mm::kCrt) ksplit = 1;
+    if (form != mm::kFp64 || chunked) tile_m = 128;  // the 64-row tile is an FP64 whole-multiply option
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
     printf("mmb one-GPU emulation: ranks=%d rows/rank=%d form=%s%s input=%s B-structure=%s", nRanks, mi,
            form_name.c_str(), mm::form_count(form, splits).c_str(), input_name.c_str(), chunked ? "K-chunked" : "single");
@@ -147,7 +149,7 @@ int main(int argc, char *argv[])
                     if (rc < 0) return rc;
                 }
             } else {
-                const int rc = mm::block_gemm(form, splits, ksplit, ws, A_r, d_B, C_r, mi, n, k, k, n, n, 0, stream);
+                const int rc = mm::block_gemm(form, splits, ksplit, ws, A_r, d_B, C_r, mi, n, k, k, n, n, 0, stream, tile_m);
                 if (rc < 0) return rc;
             }
         }
@@ -221,6 +223,7 @@ int main(int argc, char *argv[])
            input_name.c_str());
     printf("%s", mm::form_count(form, splits).c_str());
     if (ksplit > 1) printf(" ksplit=%d", ksplit);
+    if (tile_m != 128) printf(" tile_m=%d", tile_m);
     if (input != mm::kConst) printf(" norm_rel_err=%.3e max_rel_err=%.3e", err.normwise, err.max_rel);
     printf("\n");
     fflush(stdout);

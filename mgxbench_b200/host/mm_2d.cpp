@@ -109,8 +109,9 @@ int main(int argc, char **argv)
     if (input < 0 || form < 0) fail("MGXBENCH_INPUT must be const|uniform|wide and MGXBENCH_FORM fp64|ozaki|crt|auto");
     int splits = mm::env_int("MGXBENCH_SPLITS", 8);
     int ksplit = 1;  // the SUMMA panels are the K split
+    int tile_m = 128;  // the SUMMA plan's work list is of 128 x 128 tiles
     const bool autotuned = form == mm::kAuto;
-    mm::resolve_auto_form(&form, &splits, &ksplit, &form_name, M, Ncols, K,
+    mm::resolve_auto_form(&form, &splits, &ksplit, &tile_m, &form_name, M, Ncols, K,
                           input == mm::kWide ? mm::env_int("MGXBENCH_EXP_RANGE", 20) : 0, 2, true);
     if (form == mm::kCrt && !autotuned) splits = mm::env_int("MGXBENCH_MODULI", mgx_crt_choose_moduli(K, 1e-15));
     // the persistent SUMMA kernel runs the FP64 and digit-slice forms; the CRT form runs one

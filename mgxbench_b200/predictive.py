@@ -75,7 +75,7 @@ def rank_candidates(model, algorithm, m, n, k, exp_range, target, grid=(1, 1), b
     extrapolated = not all(TRAIN_LO <= d <= TRAIN_HI for d in (m, n, k))
     out = []
     for (t, e), c in zip(pred, cands):
-        out.append({"library": library, "form": c.form, "tile": c.tile,
+        out.append({"library": library, "form": c.form, "tile": c.tile, "tile_m": c.tile_m,
                     "ksplit": c.ksplit, "splits": c.splits, "grid_rows": grid[0], "grid_cols": grid[1], "summa_bk": bk,
                     "predicted_s": float(t), "predicted_error": float(e), "meets_target": bool(e <= target),
                     "algorithm": algorithm, "extrapolated": extrapolated})
@@ -92,7 +92,7 @@ def _measure(args, best, root):
         raise ValueError(f"executable not found: {exe}")
     env = dict(os.environ, MGXBENCH_EMULATED_RANKS=str(args.ranks), MGXBENCH_FORM=best["form"],
                MGXBENCH_SPLITS=str(max(best["splits"], 2)), MGXBENCH_MODULI=str(max(best["splits"], 8)),
-               MGXBENCH_KSPLIT=str(best["ksplit"]),
+               MGXBENCH_KSPLIT=str(best["ksplit"]), MGXBENCH_TILE_M=str(best.get("tile_m", 128)),
                MGXBENCH_INNER_LOOPS=str(args.repeats),
                MGXBENCH_INTERNAL_WARMUP=str(args.warmup))
     er = getattr(args, "exp_range", 0) or 0
@@ -172,6 +172,7 @@ def auto(args):
           f"\n  Splits            : {best['splits'] if best['form'] != 'fp64' else 'N/A'}"
           f"{' (moduli)' if best['form'] == 'crt' else ''}"
           f"\n  K slices          : {best['ksplit']}"
+          f"\n  Tile              : {best.get('tile_m', 128) if best['form'] == 'fp64' else (256 if best['form'] == 'crt' else 128)} x {256 if best['form'] == 'crt' else 128}"
           f"\n  SUMMA BK          : {bk if args.decomposition == '2d' else 'N/A'}"
           f"\n  Predicted Time    : {best['predicted_s']:.6f} s"
           f"\n  Predicted Error   : {best['predicted_error']:.3e} (target {target:.1e})"
