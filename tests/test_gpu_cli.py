@@ -52,6 +52,17 @@ def test_mm1d_ozaki_random_inputs():
     assert rec["valid"] == "1" and float(rec["norm_rel_err"]) <= 1e-15
 
 
+def test_mm1d_small_fp64_tile():
+    """MGXBENCH_TILE_M=64: the FP64 form with 64 x 128 output tiles, reported in the record, with
+    the same accuracy record as the default tile (the results are bit-identical)."""
+    base = launch("mm_1d", 1, 1024, "MMM", MGXBENCH_INPUT="wide", MGXBENCH_CHECK_ROWS=64)
+    small = launch("mm_1d", 1, 1024, "MMM", MGXBENCH_INPUT="wide", MGXBENCH_CHECK_ROWS=64, MGXBENCH_TILE_M=64)
+    assert base.returncode == 0 and small.returncode == 0, small.stdout + small.stderr
+    rb, rs = parse_result(base.stdout), parse_result(small.stdout)
+    assert rs["valid"] == "1" and rs["tile_m"] == "64" and "tile_m" not in rb
+    assert rs["norm_rel_err"] == rb["norm_rel_err"] and rs["max_rel_err"] == rb["max_rel_err"]
+
+
 @pytest.mark.parametrize("exe,ranks,n,env", [("mm_1d", 2, 1024, {}), ("mm_1d", 3, 1536, {"MGXBENCH_BATCH": 0}),
                                               ("mm_2d", 6, 1536, {}), ("mm_2d", 15, 1000, {"MGXBENCH_UNEVEN": 1})])
 def test_crt_form_random_inputs(exe, ranks, n, env):

@@ -210,3 +210,42 @@ def test_small_tile_beta_one_and_odd_pitch(mgx, oracle):
     assert torch.equal(c64.view(torch.int64), c128.view(torch.int64))
     ref = C0 + oracle.ab_multiply(np.ascontiguousarray(A), np.ascontiguousarray(B))
     assert np.all(np.abs(host(c64) - ref) <= 2 * gamma(k + 1) * (np.abs(A) @ np.abs(B) + np.abs(C0)))
+
+
+@pytest.mark.parametrize("m,n,k,ksplit", [(1, 1, 1, 1), (65, 129, 300, 1), (64, 128, 32, 1), (333, 127, 1000, 4),
+                                          (1024, 1024, 1024, 1), (1024, 1024, 1024, 2), (2200, 300, 200, 1),
+                                          (130, 260, 4096, 8)])
+def test_small_tile_is_bit_identical_to_the_default_tile(mgx, oracle, m, n, k, ksplit):
+    """64 x 128 output tiles (mgx_gemm_fp64_tiled, tile_m = 64) reduce every element over K in the
+    same order as the 128 x 128 tiles: the results are identical, whole-K and split-K, and inside
+    the oracle's bound."""
+    import torch
+    rng = np.random.default_rng(m + n + k + ksplit)
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    dA, dB = dev(A), dev(B)
+    c64 = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    c128 = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_fp64(dA, dB, c64, ksplit=ksplit, tile_m=64)
+    mgx.gemm_fp64(dA, dB, c128, ksplit=ksplit)
+    assert torch.equal(c64.view(torch.int64), c128.view(torch.int64))
+    check_close(host(c64), A, B, oracle, k)
+    assert mgx.device_status() == 0
+
+
+def test_small_tile_beta_one_and_odd_pitch(mgx, oracle):
+    """beta = 1 and operands that need the even-pitch copy (odd leading dimensions) through the
+    64-row tile."""
+    import torch
+    rng = np.random.default_rng(5)
+    m, n, k = 150, 100, 300          # leading dimensions 301 and 101
+    Ab, Bb = rng_matrix(rng, (m, k + 1)), rng_matrix(rng, (k, n + 1))
+    A, B = Ab[:, :k], Bb[:, :n]
+    C0 = rng_matrix(rng, (m, n))
+    dAb, dBb = dev(Ab), dev(Bb)
+    dA, dB = dAb[:, :k], dBb[:, :n]
+    c64, c128 = dev(C0), dev(C0)
+    mgx.gemm_fp64(dA, dB, c64, beta_one=True, tile_m=64)
+    mgx.gemm_fp64(dA, dB, c128, beta_one=True)
+    assert torch.equal(c64.view(torch.int64), c128.view(torch.int64))
+    ref = C0 + oracle.ab_multiply(np.ascontiguousarray(A), np.ascontiguousarray(B))
+    assert np.all(np.abs(host(c64) - ref) <= 2 * gamma(k + 1) * (np.abs(A) @ np.abs(B) + np.abs(C0)))
