@@ -394,9 +394,9 @@ def run_ours(args):
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "TFLOP/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
 
-    # CRT: scale_split_a, col_stats, col_scale, split_b, crt_gemm, crt_combine;
+    # CRT: row_scale, col_max, col_sumsq, col_scale, split_a, split_b, crt_gemm, crt_combine;
     # slices: row_exp, col_max, col_exp, split_a, split_b, ozaki_gemm
-    launches_per_step = 6
+    launches_per_step = 8 if crt else 6
     line = {
         "metric": METRIC, "value": value if valid else 0.0, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,

@@ -351,7 +351,7 @@ def gemm_host(hA, hB, hC, form=FORM_OZAKI, splits=8, panels=32, stream=None):
 # Kernel launches of one product per K chunk of one exact int32 accumulation: the FP64 SUMMA
 # plan's persistent kernel; the slice form's exponent, digit and product kernels; the CRT form's
 # scale, residue, product and recombination kernels.
-_LAUNCHES_PER_CHUNK = {FORM_FP64: 1, FORM_OZAKI: 6, FORM_CRT: 6}
+_LAUNCHES_PER_CHUNK = {FORM_FP64: 1, FORM_OZAKI: 6, FORM_CRT: 8}
 
 
 def launches_per_product(form: int, k: int, splits: int = 0) -> int:

@@ -13,11 +13,8 @@
 //   scale    row i of A: e = frexp exponent of max|a_ik|, c_k = max(1, ceil(|a_ik| 2^(22-e))) for
 //            a_ik != 0, S = sum c_k^2 (an integer sum, so the result does not depend on the
 //            order), u = (bitlen(S-1)+1)/2, sigma_i = alpha - e + 22 - u; then 2^sigma_i ||a_i||
-//            <= 2^alpha.  Columns of B likewise (tau_j, beta), except that S is summed in chunks
-//            of 256 rows, each relative to its own maximum exponent e_c, and combined as
-//            S = sum_c ceil(S_c / 4^(e - e_c)) -- still an upper bound, still order-free, and
-//            computable in one pass over B.  By Cauchy-Schwarz the exact product C'_ij of
-//            A' = rint(2^sigma A) and B' = rint(B 2^tau) is below P/4.
+//            <= 2^alpha.  Columns of B likewise (tau_j, beta).  By Cauchy-Schwarz the exact
+//            product C'_ij of A' = rint(2^sigma A) and B' = rint(B 2^tau) is below P/4.
 //   residues A' mod p_l as int8 (symmetric; [-128, 127] for 256), B' likewise.
 //   products R_l = (A'_l B'_l) mod p_l in [0, p_l), exact in int32 while K <= 130816.
 //   CRT      w_l = (P/p_l) ((P/p_l)^-1 mod p_l) in three 40-bit chunks; s_t = sum_l w_t,l R_l is
@@ -25,11 +22,9 @@
 //            C_ij = fma(fma(d1, 2^40, d2), 2^40, d3) 2^(E3 - sigma_i - tau_j).
 //
 // Kernels:
-//   crt_scale_split_a   one block per row of A: sigma (maximum, integer sum of squares) and the
-//                       row's residues as swizzled K-major 256-row slabs [modulus][tile][K block];
-//                       the second and third passes over the row hit L2, so A leaves DRAM once
-//   crt_col_stats / crt_col_scale   tau per column of B from one pass over B: the maximum and the
-//                       integer sum of squares of every 256-row chunk, combined exactly
+//   crt_row_scale   sigma per row of A (one block per row, integer sum of squares)
+//   crt_col_max / crt_col_sumsq / crt_col_scale   tau per column of B (integer atomics)
+//   crt_split_a     residues of A as swizzled K-major 256-row slabs [modulus][tile][K block]
 //   crt_split_b     residues of B^T, same layout (thread per column, coalesced reads)
 //   crt_gemm        persistent tcgen05 kernel over (modulus, 256 x 256 tile) work items:
 //       warp 0      producer: one bulk copy per operand per stage (KPACK K blocks); at each new
@@ -141,67 +136,108 @@ __device__ __forceinline__ int sigma_of(unsigned long long mx, unsigned long lon
 }
 
 // ---------------------------------------------------------------- scale kernels
-// Column statistics of B in one pass.  Block (column block, chunk): each thread takes one column
-// (so a warp reads 256 contiguous bytes per row) over the chunk's COL_CHUNK rows, finds the
-// chunk maximum, then sums max(1, ceil(|b| 2^(22 - e_c)))^2 over the chunk (the second pass finds
-// the block's 256 x 256 x 8 B in L1/L2).  Chunk c of column j goes to cmax / csum[c * ld + j].
-constexpr int COL_CHUNK = 256;
+// One block of ROW_THREADS per row: the row's maximum, then its integer sum of squares.  The
+// second pass finds the row in L2: at 4 blocks per SM, 592 rows (77 MB at k = 16384) are in
+// flight, against L2's 126 MB, so A is read from DRAM once.
+constexpr int ROW_THREADS = 512;
 
-__global__ void __launch_bounds__(256) crt_col_stats(const double *__restrict__ B, int k, int n, int ldb, size_t ld,
-                                                     unsigned long long *__restrict__ cmax,
-                                                     unsigned long long *__restrict__ csum)
+__global__ void __launch_bounds__(ROW_THREADS) crt_row_scale(const double *__restrict__ A, int m, int k, int lda,
+                                                             int target, int *__restrict__ sg, int *status)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const int r0 = blockIdx.y * COL_CHUNK;
-    const int r1 = min(k, r0 + COL_CHUNK);
-    const unsigned long long *b = reinterpret_cast<const unsigned long long *>(B) + j;
+    __shared__ unsigned long long red[ROW_THREADS / 32];
+    __shared__ unsigned long long row_max;
+    const int row = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (row >= m) return;
+    const double *r = A + (size_t)row * lda;
+    const unsigned long long *rb = reinterpret_cast<const unsigned long long *>(r);
     unsigned long long mx = 0;
-#pragma unroll 8
-    for (int r = r0; r < r1; ++r) {
-        const unsigned long long v = __ldg(b + (size_t)r * ldb) & 0x7fffffffffffffffull;
-        mx = v > mx ? v : mx;
+    for (int kk = threadIdx.x; kk < k; kk += ROW_THREADS) {
+        const unsigned long long b = __ldg(rb + kk) & 0x7fffffffffffffffull;
+        mx = b > mx ? b : mx;
     }
-    unsigned long long S = 0;
-    if (mx != 0 && mx < 0x7ff0000000000000ull) {
-        const int e = frexp_exp_bits(mx);
-#pragma unroll 8
-        for (int r = r0; r < r1; ++r) S += sq_term(__ldg(B + (size_t)r * ldb + j), e);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = other > mx ? other : mx;
     }
-    cmax[(size_t)blockIdx.y * ld + j] = mx;
-    csum[(size_t)blockIdx.y * ld + j] = S;
-}
-
-// tau per column from its chunks: e from the column maximum, S = sum_c ceil(S_c / 4^(e - e_c)).
-__global__ void crt_col_scale(const unsigned long long *__restrict__ cmax, const unsigned long long *__restrict__ csum,
-                              int chunks, size_t ld, int n, int target, int *__restrict__ tu, int *status)
-{
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    unsigned long long mx = 0;
-    for (int c = 0; c < chunks; ++c) {
-        const unsigned long long v = cmax[(size_t)c * ld + j];
-        mx = v > mx ? v : mx;
+    if (lane == 0) red[warp] = mx;
+    __syncthreads();
+    if (warp == 0) {
+        mx = lane < ROW_THREADS / 32 ? red[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, mx, o);
+            mx = other > mx ? other : mx;
+        }
+        if (lane == 0) row_max = mx;
     }
+    __syncthreads();
+    mx = row_max;
     if (mx >= 0x7ff0000000000000ull) {
-        tu[j] = NONFINITE;
-        record_status(status, kDevNonFinite);
-        return;
-    }
-    if (mx == 0) {
-        tu[j] = 0;
+        if (threadIdx.x == 0) {
+            sg[row] = NONFINITE;
+            record_status(status, kDevNonFinite);
+        }
         return;
     }
     const int e = frexp_exp_bits(mx);
     unsigned long long S = 0;
-    for (int c = 0; c < chunks; ++c) {
-        const unsigned long long v = cmax[(size_t)c * ld + j];
-        if (v == 0) continue;
-        const int sh = 2 * (e - frexp_exp_bits(v));
-        const unsigned long long sc = csum[(size_t)c * ld + j];
-        S += sh >= 64 ? 1ull : (sc + ((1ull << sh) - 1ull)) >> sh;
+    if (mx != 0)
+        for (int kk = threadIdx.x; kk < k; kk += ROW_THREADS) S += sq_term(__ldg(r + kk), e);
+    for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
+    if (lane == 0) red[warp] = S;   // warp 0 read red[] before the barrier above
+    __syncthreads();
+    if (warp == 0) {
+        S = lane < ROW_THREADS / 32 ? red[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
+        if (lane == 0) sg[row] = sigma_of(mx, S, target);
     }
-    tu[j] = sigma_of(mx, S, target);
+}
+
+// grid (ceil(n/256), ychunks); each thread scans a run of rows of one column.
+__global__ void crt_col_max(const double *__restrict__ B, int k, int n, int ldb, unsigned long long *colmax)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int rows_per = (k + gridDim.y - 1) / gridDim.y;
+    const int r0 = blockIdx.y * rows_per;
+    const int r1 = min(k, r0 + rows_per);
+    unsigned long long mx = 0;
+    const unsigned long long *b = reinterpret_cast<const unsigned long long *>(B);
+    for (int r = r0; r < r1; ++r) {
+        const unsigned long long v = __ldg(b + (size_t)r * ldb + j) & 0x7fffffffffffffffull;
+        mx = v > mx ? v : mx;
+    }
+    if (mx) atomicMax(colmax + j, mx);
+}
+
+__global__ void crt_col_sumsq(const double *__restrict__ B, int k, int n, int ldb,
+                              const unsigned long long *__restrict__ colmax, unsigned long long *colsum)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long mx = colmax[j];
+    if (mx == 0 || mx >= 0x7ff0000000000000ull) return;
+    const int e = frexp_exp_bits(mx);
+    const int rows_per = (k + gridDim.y - 1) / gridDim.y;
+    const int r0 = blockIdx.y * rows_per;
+    const int r1 = min(k, r0 + rows_per);
+    unsigned long long S = 0;
+    for (int r = r0; r < r1; ++r) S += sq_term(__ldg(B + (size_t)r * ldb + j), e);
+    if (S) atomicAdd(colsum + j, S);
+}
+
+__global__ void crt_col_scale(const unsigned long long *__restrict__ colmax, const unsigned long long *__restrict__ colsum,
+                              int n, int target, int *__restrict__ tu, int *status)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long mx = colmax[j];
+    if (mx >= 0x7ff0000000000000ull) {
+        tu[j] = NONFINITE;
+        record_status(status, kDevNonFinite);
+    } else {
+        tu[j] = sigma_of(mx, colsum[j], target);
+    }
 }
 
 // ---------------------------------------------------------------- residue kernels
@@ -273,89 +309,37 @@ __device__ __forceinline__ size_t slab_offset(int tile, int kb, int kblocks, int
     return ((size_t)tile * kblocks + kb) * (size_t)SLAB + (size_t)r * 32 + (c ^ (((r >> 2) & 1) << 4));
 }
 
-// One block of SA_THREADS per row of A (rows m..mp-1 are the tile padding, written as zero
-// residues): the row's maximum, its integer sum of squares, sigma, then its residues.  The first
-// pass reads the row from DRAM; the second and third find it in L2 (3 blocks per SM keep 444
-// rows, 58 MB at k = 16384, in flight against 126 MB of L2), so A is read from DRAM once.  In
-// the residue pass each thread splits 8 consecutive k and writes their 8 bytes per modulus to
-// the row's 32-byte line of the K block's slab; the 4 or 8 rows that share a 128-byte line are
-// in flight together, so L2 merges their stores before write-back.  The stores are marked
-// streaming (evict first), so they do not push the rows still being read out of L2.
-constexpr int SA_THREADS = 256;
-
+// Block: 64 rows of A x one 32-wide K block; warp w takes rows 8w..8w+7, lane -> row (lane / 4)
+// and 8 consecutive k (lane % 4), so four lanes read one 256-byte row segment and write the 32
+// residue bytes of that row, one 8-byte store each per modulus.
 template <int Q>
-__global__ void __launch_bounds__(SA_THREADS, 3) crt_scale_split_a(const double *__restrict__ A, int m, int k, int lda,
-                                                                   int kblocks, int target, int *__restrict__ sg,
-                                                                   uint8_t *__restrict__ ra, size_t mod_stride,
-                                                                   const __grid_constant__ Consts K, int *status)
+__global__ void __launch_bounds__(256, 3) crt_split_a(const double *__restrict__ A, int m, int k, int lda, int mp,
+                                                      int kblocks, const int *__restrict__ sg, uint8_t *__restrict__ ra,
+                                                      size_t mod_stride, const __grid_constant__ Consts K)
 {
-    __shared__ unsigned long long red[SA_THREADS / 32];
-    __shared__ int row_sigma;
-    const int row = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const double *r = A + (size_t)(row < m ? row : 0) * lda;
-    int s = NONFINITE;
-    if (row < m) {
-        const unsigned long long *rb = reinterpret_cast<const unsigned long long *>(r);
-        unsigned long long mx = 0;
-#pragma unroll 4
-        for (int kk = threadIdx.x; kk < k; kk += SA_THREADS) {
-            const unsigned long long b = __ldg(rb + kk) & 0x7fffffffffffffffull;
-            mx = b > mx ? b : mx;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(0xffffffffu, mx, o);
-            mx = other > mx ? other : mx;
-        }
-        if (lane == 0) red[warp] = mx;
-        __syncthreads();
-        mx = 0;
-#pragma unroll
-        for (int w = 0; w < SA_THREADS / 32; ++w) mx = red[w] > mx ? red[w] : mx;
-        __syncthreads();  // every thread has read red[] before it is reused
-        if (mx < 0x7ff0000000000000ull) {
-            const int e = frexp_exp_bits(mx);
-            unsigned long long S = 0;
-            if (mx != 0)
-#pragma unroll 4
-                for (int kk = threadIdx.x; kk < k; kk += SA_THREADS) S += sq_term(__ldg(r + kk), e);
-            for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
-            if (lane == 0) red[warp] = S;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                S = 0;
-#pragma unroll
-                for (int w = 0; w < SA_THREADS / 32; ++w) S += red[w];
-                row_sigma = sigma_of(mx, S, target);
-                sg[row] = row_sigma;
-            }
-        } else if (threadIdx.x == 0) {
-            row_sigma = NONFINITE;
-            sg[row] = NONFINITE;
-            record_status(status, kDevNonFinite);
-        }
-        __syncthreads();
-        s = row_sigma;
-    }
-    const bool live = s != NONFINITE;
+    const int kb = blockIdx.y;
+    const int row = blockIdx.x * 64 + warp * 8 + (lane >> 2), kq = lane & 3;
+    if (row >= mp) return;
+    const int k0 = kb * 32 + kq * 8;
+    int s = (row < m) ? sg[row] : 0;
+    const bool live = row < m && s != NONFINITE;
     if (!live) s = 0;
     double f1, f2;
     scale_factors(s, f1, f2);
-    const int tile = row / TILE, trow = row % TILE;
-    for (int k0 = threadIdx.x * 8; k0 < kblocks * 32; k0 += SA_THREADS * 8) {
-        double xh[8], xr[8];
+    const double *arow = A + (size_t)(live ? row : 0) * lda;
+    double xh[8], xr[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int kk = k0 + j;
-            double v = (live && kk < k) ? __ldg(r + kk) : 0.0;
-            if (!isfinite(v)) v = 0.0;
-            split32(v, f1, f2, xh[j], xr[j]);
-        }
-        const size_t off = slab_offset(tile, k0 >> 5, kblocks, trow, k0 & 31);
-#pragma unroll
-        for (int l = 0; l < Q; ++l)
-            __stcs(reinterpret_cast<uint2 *>(ra + (size_t)l * mod_stride + off), residues8(xh, xr, K, l));
+    for (int j = 0; j < 8; ++j) {
+        const int kk = k0 + j;
+        double v = (live && kk < k) ? __ldg(arow + kk) : 0.0;
+        if (!isfinite(v)) v = 0.0;
+        split32(v, f1, f2, xh[j], xr[j]);
     }
+    const size_t off = slab_offset(row / TILE, kb, kblocks, row % TILE, kq * 8);
+#pragma unroll
+    for (int l = 0; l < Q; ++l)
+        *reinterpret_cast<uint2 *>(ra + (size_t)l * mod_stride + off) = residues8(xh, xr, K, l);
 }
 
 // Block: 64 consecutive columns of B x one 32-wide K block.  Warp w takes 32 of the columns
@@ -850,7 +834,6 @@ struct CrtLayout {
     size_t ra_mod, rb_mod, rc_mod;
     int kblocks, tiles_m, tiles_n;
     int ksplit, kb_split;   // K slices (1: whole K) and K blocks per slice
-    int ncols, col_chunks;  // columns of B, and 256-row chunks of its column statistics
 };
 
 // Workspace of one K range of at most KMAX: residue slabs of A and B^T (rows rounded up to 256,
@@ -883,14 +866,10 @@ CrtLayout crt_layout(int m, int n, int k, int q, int ksplit = 1)
     off = align256(off + sizeof(int) * (size_t)m);
     L.tu = off;
     off = align256(off + sizeof(int) * (size_t)n);
-    // per-chunk column statistics: [chunk][column], COL_CHUNK rows per chunk
-    L.ncols = n;
-    L.col_chunks = (kc + crt::COL_CHUNK - 1) / crt::COL_CHUNK;
-    if (L.col_chunks < 1) L.col_chunks = 1;
     L.colmax = off;
-    off = align256(off + sizeof(unsigned long long) * (size_t)n * L.col_chunks);
+    off = align256(off + sizeof(unsigned long long) * (size_t)n);
     L.colsum = off;
-    off = align256(off + sizeof(unsigned long long) * (size_t)n * L.col_chunks);
+    off = align256(off + sizeof(unsigned long long) * (size_t)n);
     L.sync = off;                       // arrival counters of the products launches (two slots)
     off = align256(off + 2 * sizeof(unsigned int));
     L.total = off;
@@ -917,13 +896,13 @@ int dispatch_q(int q, Args... args)
 }
 
 template <int Q>
-struct ScaleSplitA {
-    static int run(const double *A, int m, int k, int lda, const CrtLayout &L, int *sg, uint8_t *ra,
+struct SplitA {
+    static int run(const double *A, int m, int k, int lda, const CrtLayout &L, const int *sg, uint8_t *ra,
                    const crt::Consts &K, cudaStream_t stream)
     {
-        const int rows = ((m + crt::TILE - 1) / crt::TILE) * crt::TILE;
-        crt::crt_scale_split_a<Q><<<rows, crt::SA_THREADS, 0, stream>>>(A, m, k, lda, L.kblocks, K.alpha, sg, ra,
-                                                                        L.ra_mod, K, mgx_device_status_ptr());
+        const int tiles = (m + crt::TILE - 1) / crt::TILE;
+        crt::crt_split_a<Q><<<dim3(tiles * 4, L.kblocks), 256, 0, stream>>>(A, m, k, lda, tiles * crt::TILE,
+                                                                            L.kblocks, sg, ra, L.ra_mod, K);
         MGX_HOST_CHECK(cudaGetLastError());
         return MGX_SUCCESS;
     }
@@ -962,27 +941,35 @@ int crt_split_a_impl(const double *A, int m, int k, int lda, int r0, const crt::
                      const CrtLayout &L, cudaStream_t stream)
 {
     if (m <= 0) return MGX_SUCCESS;
+    int *status = mgx_device_status_ptr();
     int *sg = reinterpret_cast<int *>(ws + L.sg) + r0;
     uint8_t *ra = ws + L.ra + (size_t)(r0 / crt::TILE) * L.kblocks * crt::SLAB;
-    return dispatch_q<ScaleSplitA>(K.q, A, m, k, lda, L, sg, ra, K, stream);
+    crt::crt_row_scale<<<m, crt::ROW_THREADS, 0, stream>>>(A, m, k, lda, K.alpha, sg, status);
+    MGX_HOST_CHECK(cudaGetLastError());
+    return dispatch_q<SplitA>(K.q, A, m, k, lda, L, (const int *)sg, ra, K, stream);
 }
 
-// The same for columns [c0, c0 + n) of B (k x n): the chunk statistics of one pass over B, the
-// scales, then the residues.
+// The same for columns [c0, c0 + n) of B (k x n).
 int crt_split_b_impl(const double *B, int n, int k, int ldb, int c0, const crt::Consts &K, unsigned char *ws,
                      const CrtLayout &L, cudaStream_t stream)
 {
     if (n <= 0) return MGX_SUCCESS;
     int *status = mgx_device_status_ptr();
     int *tu = reinterpret_cast<int *>(ws + L.tu) + c0;
-    unsigned long long *cmax = reinterpret_cast<unsigned long long *>(ws + L.colmax) + c0;
-    unsigned long long *csum = reinterpret_cast<unsigned long long *>(ws + L.colsum) + c0;
+    unsigned long long *colmax = reinterpret_cast<unsigned long long *>(ws + L.colmax) + c0;
+    unsigned long long *colsum = reinterpret_cast<unsigned long long *>(ws + L.colsum) + c0;
     uint8_t *rb = ws + L.rb + (size_t)(c0 / crt::TILE) * L.kblocks * crt::SLAB;
-    const int chunks = (k + crt::COL_CHUNK - 1) / crt::COL_CHUNK;
-    crt::crt_col_stats<<<dim3((n + 255) / 256, chunks), 256, 0, stream>>>(B, k, n, ldb, (size_t)L.ncols, cmax, csum);
+    MGX_HOST_CHECK(cudaMemsetAsync(colmax, 0, sizeof(unsigned long long) * (size_t)n, stream));
+    MGX_HOST_CHECK(cudaMemsetAsync(colsum, 0, sizeof(unsigned long long) * (size_t)n, stream));
+    const int sms = mgx_sm_count();
+    int ych = (sms * 8) / ((n + 255) / 256);
+    if (ych > (k + 63) / 64) ych = (k + 63) / 64;
+    if (ych < 1) ych = 1;
+    crt::crt_col_max<<<dim3((n + 255) / 256, ych), 256, 0, stream>>>(B, k, n, ldb, colmax);
     MGX_HOST_CHECK(cudaGetLastError());
-    crt::crt_col_scale<<<(n + 255) / 256, 256, 0, stream>>>(cmax, csum, chunks, (size_t)L.ncols, n, K.beta, tu,
-                                                            status);
+    crt::crt_col_sumsq<<<dim3((n + 255) / 256, ych), 256, 0, stream>>>(B, k, n, ldb, colmax, colsum);
+    MGX_HOST_CHECK(cudaGetLastError());
+    crt::crt_col_scale<<<(n + 255) / 256, 256, 0, stream>>>(colmax, colsum, n, K.beta, tu, status);
     MGX_HOST_CHECK(cudaGetLastError());
     return dispatch_q<SplitB>(K.q, B, n, k, ldb, L, (const int *)tu, rb, K, stream);
 }

@@ -703,11 +703,6 @@ ORACLE_API int oracle_ozaki_gemm_splitk(const double *A, const double *B, double
  *            for a_ik != 0; S = sum c_k^2 (uint64, so independent of the order);
  *            u = ceil(log2(S) / 2) = (bitlen(S - 1) + 1) / 2; sigma_i = alpha - e + 22 - u, so
  *            2^sigma_i ||a_i||_2 <= 2^alpha.  Columns of B likewise with beta.
- *            Columns of B sum in chunks of CRT_COL_CHUNK rows: chunk c has its own maximum
- *            exponent e_c and S_c = sum max(1, ceil(|b| 2^(22-e_c)))^2; the column's
- *            S = sum_c ceil(S_c / 2^(2(e - e_c))) (each term an integer upper bound of the
- *            chunk's share, so S still bounds sum (|b| 2^(22-e))^2 and does not depend on the
- *            order of the chunks).  The GPU reads B once for all chunk sums this way.
  *            alpha = (L - 3) / 2, beta = L - 3 - alpha: by Cauchy-Schwarz every exact integer
  *            product C'_ij = sum_k A'_ik B'_kj of the scaled, rounded operands
  *            A' = rint(2^sigma A), B' = rint(B 2^tau) has |C'_ij| < P / 4.
@@ -802,49 +797,6 @@ static int crt_sigma(const double *v, size_t stride, int k, int target, int *non
     return target - e + 22 - u;
 }
 
-/* tau of one column of B (k values, stride ldb) from chunk sums, as described above. */
-#define CRT_COL_CHUNK 256
-static int crt_tau_chunked(const double *v, size_t stride, int k, int target, int *nonfinite)
-{
-    uint64_t mx = 0, S = 0;
-    const int chunks = (k + CRT_COL_CHUNK - 1) / CRT_COL_CHUNK;
-    uint64_t cmx[(CRT_KMAX + CRT_COL_CHUNK - 1) / CRT_COL_CHUNK], csum[(CRT_KMAX + CRT_COL_CHUNK - 1) / CRT_COL_CHUNK];
-    for (int c = 0; c < chunks; ++c) {
-        const int r0 = c * CRT_COL_CHUNK, r1 = (r0 + CRT_COL_CHUNK < k) ? r0 + CRT_COL_CHUNK : k;
-        uint64_t cm = 0, cs = 0;
-        for (int r = r0; r < r1; ++r) {
-            uint64_t b;
-            memcpy(&b, &v[(size_t)r * stride], 8);
-            b &= 0x7fffffffffffffffull;
-            if (b >= 0x7ff0000000000000ull) *nonfinite = 1;
-            if (b > cm) cm = b;
-        }
-        if (cm != 0 && cm < 0x7ff0000000000000ull) {
-            const int ec = frexp_exp_bits(cm);
-            for (int r = r0; r < r1; ++r) {
-                const double x = fabs(v[(size_t)r * stride]);
-                if (x == 0.0) continue;
-                double t = ceil(scale2(x, 22 - ec));
-                if (t < 1.0) t = 1.0;
-                const uint64_t ci = (uint64_t)t;
-                cs += ci * ci;
-            }
-        }
-        cmx[c] = cm;
-        csum[c] = cs;
-        if (cm > mx) mx = cm;
-    }
-    if (mx == 0 || mx >= 0x7ff0000000000000ull) return 0;
-    const int e = frexp_exp_bits(mx);
-    for (int c = 0; c < chunks; ++c) {
-        if (cmx[c] == 0) continue;
-        const int sh = 2 * (e - frexp_exp_bits(cmx[c]));
-        S += sh >= 64 ? 1 : (csum[c] + ((1ull << sh) - 1)) >> sh;
-    }
-    const int u = (bitlen64(S - 1) + 1) / 2;
-    return target - e + 22 - u;
-}
-
 /* Symmetric residue of the integer x (|x| < 2^63) modulo p. */
 static int8_t crt_residue(int64_t x, int p)
 {
@@ -867,7 +819,7 @@ ORACLE_API int oracle_crt_scales(const double *A, const double *B, int m, int n,
 #pragma omp parallel for schedule(dynamic, 16) reduction(| : nonfinite)
     for (int i = 0; i < m; ++i) sigma[i] = crt_sigma(A + (size_t)i * lda, 1, k, K.alpha, &nonfinite);
 #pragma omp parallel for schedule(dynamic, 16) reduction(| : nonfinite)
-    for (int j = 0; j < n; ++j) tau[j] = crt_tau_chunked(B + j, (size_t)ldb, k, K.beta, &nonfinite);
+    for (int j = 0; j < n; ++j) tau[j] = crt_sigma(B + j, (size_t)ldb, k, K.beta, &nonfinite);
     return nonfinite;
 }
 

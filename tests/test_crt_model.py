@@ -63,3 +63,4 @@ def test_barrett_reduction_of_the_epilogue():
         r = np.where(r < 0, r + p, r)
         R = np.where((g >= 0) | (r == 0), r, p - r)
         assert np.array_equal(R, np.mod(g, p)), p
+

@@ -223,53 +223,3 @@ def test_crt_oracle_against_exact_integers(oracle, q, kind, er):
             else:
                 assert abs(Fraction(float(C[i, j])) - exact) <= 2 * abs(exact) * Fraction(2) ** -53
 
-
-def _tau_chunked_exact(col, target, chunk=256):
-    """The column scale of the CRT form from chunk sums, in exact integer arithmetic: chunk c of
-    `chunk` rows has maximum exponent e_c and S_c = sum max(1, ceil(|b| 2^(22 - e_c)))^2 over its
-    nonzero entries; S = sum_c ceil(S_c / 4^(e - e_c)) with e the column maximum's exponent."""
-    import math
-    vals = [abs(Fraction(float(b))) for b in col]
-    nz = [v for v in vals if v]
-    if not nz:
-        return 0
-
-    def fexp(v):                       # frexp exponent: v = f 2^e with f in [1/2, 1)
-        e = v.numerator.bit_length() - v.denominator.bit_length()
-        while Fraction(2) ** e <= v:
-            e += 1
-        while Fraction(2) ** (e - 1) > v:
-            e -= 1
-        return e
-    e = fexp(max(nz))
-    S = 0
-    for c0 in range(0, len(vals), chunk):
-        part = [v for v in vals[c0:c0 + chunk] if v]
-        if not part:
-            continue
-        ec = fexp(max(part))
-        Sc = sum(max(1, math.ceil(v * Fraction(2) ** (22 - ec))) ** 2 for v in part)
-        S += -(-Sc // 4 ** (e - ec))
-    return target - e + 22 - ((S - 1).bit_length() + 1) // 2
-
-
-def test_crt_column_scale_from_chunk_sums(oracle):
-    """Columns longer than one 256-row chunk, with chunks of very different magnitude (and an
-    all-zero chunk): tau follows the chunked rule exactly and still bounds the column norm."""
-    import math
-    rng = np.random.default_rng(99)
-    k, n, q = 1000, 5, 15
-    B = rng_matrix(rng, (k, n), "wide", 20)
-    B[0:256, 0] *= 2.0 ** -40          # a small first chunk under a large column maximum
-    B[256:512, 1] = 0.0                # an empty chunk
-    B[700:760, 2] *= 2.0 ** 30         # the maximum in the third chunk
-    B[:, 3] *= 2.0 ** -1030            # subnormal-range column (two-step scaling)
-    A = rng_matrix(rng, (2, k))
-    _, tu, rc = oracle.crt_scales(A, B, q)
-    assert rc == 0
-    P = math.prod(CRT_MODULI[:q])
-    L = P.bit_length()
-    beta = L - 3 - (L - 3) // 2
-    for j in range(n):
-        assert int(tu[j]) == _tau_chunked_exact(B[:, j], beta), j
-        assert sum((Fraction(float(b)) * Fraction(2) ** int(tu[j])) ** 2 for b in B[:, j]) <= Fraction(4) ** beta
