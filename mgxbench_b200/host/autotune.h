@@ -5,7 +5,7 @@
 // constants (xmean, xstd, ymean, ystd), the flat parameter vector of the 6 -> 64 -> 64 -> 2 MLP
 // and the candidate list [[tile, splits], ...].  Inference runs on the GPU through
 // mgx_mlp_forward; the rule is the one of mgxbench_b200.autotune.choose: the fastest candidate
-// whose predicted normwise error meets the target (with a 1.5 guard band for the CRT form), else
+// whose predicted normwise error meets the target (with a guard band of 2 for the CRT form), else
 // the candidate with the most splits.
 // MGXBench's own AUTO mode (autotuning/predictive.py:606-657) chooses a communication library
 // from a regression of measured times; here the choice is the kernel configuration.
@@ -205,8 +205,8 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
     for (int c = 0; c < nc; ++c) {
         const double t = std::exp(Y[(size_t)c * 2] * ystd[0] + ymean[0]);
         const double e = std::pow(10.0, Y[(size_t)c * 2 + 1] * ystd[1] + ymean[1]);
-        // a CRT candidate needs a guard band of 1.5 (mgxbench_b200.autotune.CRT_ERROR_MARGIN)
-        const double guard = tile_is_crt((int)cand[2 * c]) ? 1.5 : 1.0;
+        // a CRT candidate needs a guard band of 2 (mgxbench_b200.autotune.CRT_ERROR_MARGIN)
+        const double guard = tile_is_crt((int)cand[2 * c]) ? 2.0 : 1.0;
         if (e * guard <= target && (best < 0 || t < best_t)) {
             best = c;
             best_t = t;
