@@ -127,6 +127,17 @@ MGX_API int mgx_gemm_fp64_tiled(const double *A, const double *B, double *C, int
                                 int ldc, int beta_one, int tile_m, int ksplit, void *workspace,
                                 size_t workspace_bytes, void *stream);
 
+/* Stream-K form of the FP64 product over 64 x 128 tiles, for products with too few tiles to fill
+ * the GPU (no counterpart in MGXBench; the autotuner offers it).  Every CTA takes an equal
+ * share of all tiles' 32-wide K blocks, so every SM has the same work; a tile whose K range is
+ * split between CTAs is finished by the last of them to arrive, which adds the pieces in K order.
+ * No CTA waits for another.  Deterministic for a given GPU (the shares depend on its SM count),
+ * and within the same any-order bound as the other FP64 entry points.  `workspace` (256-byte
+ * aligned) holds mgx_fp64_streamk_workspace_size(m, n, k) bytes on the current device. */
+MGX_API size_t mgx_fp64_streamk_workspace_size(int m, int n, int k);
+MGX_API int mgx_gemm_fp64_streamk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                                  int ldc, int beta_one, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------------------------------------
  * Ozaki-scheme FP64 GEMM on the INT8 tensor cores (tcgen05, exact int32 TMEM accumulation)
  * ------------------------------------------------------------------------------------------ */

@@ -64,6 +64,8 @@ EXPORTS = [
     ("mgx_fp64_splitk_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_fp64_splitk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_gemm_fp64_tiled", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
+    ("mgx_fp64_streamk_workspace_size", _sz, [_i, _i, _i]),
+    ("mgx_gemm_fp64_streamk", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_workspace_size", _sz, [_i, _i, _i, _i]),
     ("mgx_gemm_ozaki", _i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _sz, _vp]),
     ("mgx_ozaki_splitk_workspace_size", _sz, [_i, _i, _i, _i, _i]),
@@ -189,10 +191,18 @@ def fp64_splitk_workspace_size(m, n, k, ksplit) -> int:
 def gemm_fp64(A, B, C, beta_one: bool = False, stream=None, ksplit: int = 1, workspace=None, tile_m: int = 128):
     """C (+)= A B on the FP64 tensor cores; ksplit > 1 cuts K into slices computed by separate
     CTAs (for products with few output tiles) and needs a workspace (grown on demand); tile_m = 64
-    runs 64 x 128 output tiles instead of 128 x 128 (same result, bit for bit)."""
+    runs 64 x 128 output tiles instead of 128 x 128 (same result, bit for bit); ksplit = 0 is the
+    stream-K form over 64 x 128 tiles (equal K shares per CTA, workspace grown on demand)."""
     _check_f64(A, B, C)
     m, k = A.shape
     n = B.shape[1]
+    if ksplit == 0:
+        # stream-K over 64 x 128 tiles
+        need = lib().mgx_fp64_streamk_workspace_size(m, n, k)
+        ws = (workspace or _default_ws).get(need) if need else None
+        return _check(lib().mgx_gemm_fp64_streamk(_ptr(A), _ptr(B), _ptr(C), m, n, k, _ld(A), _ld(B), _ld(C),
+                                                  int(beta_one), _ptr(ws), ws.numel() if ws is not None else 0,
+                                                  _stream(stream)), "mgx_gemm_fp64_streamk")
     if tile_m != 128:
         need = fp64_splitk_workspace_size(m, n, k, ksplit) if ksplit > 1 else 0
         ws = (workspace or _default_ws).get(need) if need else None

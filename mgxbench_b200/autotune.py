@@ -41,9 +41,14 @@ TILE_CRT = 8
 # native FP64 kernel, 64 x 128 output tiles (twice the work items of the 128 x 128 tile), over the
 # whole K range or cut into 2 / 4 / 8 slices
 TILE_FP64_T64, TILE_FP64_T64_K2, TILE_FP64_T64_K4, TILE_FP64_T64_K8 = 9, 10, 11, 12
+# native FP64 kernel, 64 x 128 output tiles, stream-K: every CTA an equal share of all tiles' K
+# blocks (its "ksplit" is 0)
+TILE_FP64_T64_SK = 13
 FP64_KSPLIT = {TILE_FP64: 1, TILE_FP64_K2: 2, TILE_FP64_K4: 4, TILE_FP64_K8: 8, TILE_FP64_K16: 16,
-               TILE_FP64_T64: 1, TILE_FP64_T64_K2: 2, TILE_FP64_T64_K4: 4, TILE_FP64_T64_K8: 8}
-FP64_TILE_M = {TILE_FP64_T64: 64, TILE_FP64_T64_K2: 64, TILE_FP64_T64_K4: 64, TILE_FP64_T64_K8: 64}
+               TILE_FP64_T64: 1, TILE_FP64_T64_K2: 2, TILE_FP64_T64_K4: 4, TILE_FP64_T64_K8: 8,
+               TILE_FP64_T64_SK: 0}
+FP64_TILE_M = {TILE_FP64_T64: 64, TILE_FP64_T64_K2: 64, TILE_FP64_T64_K4: 64, TILE_FP64_T64_K8: 64,
+               TILE_FP64_T64_SK: 64}
 OZAKI_KSPLIT = {TILE_OZAKI_128: 1, TILE_OZAKI_K4: 4, TILE_OZAKI_K16: 16}
 SPLITS = tuple(range(3, 10))
 CRT_MODULI = (9, 11, 12, 13, 14, 15, 16)
@@ -76,7 +81,10 @@ class Candidate:
 
     @property
     def ksplit(self) -> int:
-        return FP64_KSPLIT.get(self.tile) or OZAKI_KSPLIT.get(self.tile, 1)
+        """K slices (1: whole K; 0: the FP64 stream-K schedule)."""
+        if self.tile in FP64_KSPLIT:
+            return FP64_KSPLIT[self.tile]
+        return OZAKI_KSPLIT.get(self.tile, 1)
 
     @property
     def tile_m(self) -> int:
@@ -86,6 +94,8 @@ class Candidate:
     @property
     def name(self) -> str:
         base = ("fp64" if self.tile_m == 128 else "fp64t64") if self.is_fp64 else f"{self.form}{self.splits}"
+        if self.ksplit == 0:
+            return base + "sk"
         return base if self.ksplit == 1 else f"{base}k{self.ksplit}"
 
 
@@ -101,7 +111,7 @@ def splitk_applies(m, n, k, ksplit, splits=0):
     """A split-K candidate is offered when every slice gets a 32-wide K block and the partial
     products fit SPLITK_WORKSPACE_LIMIT; an Ozaki one also needs K within one int32 accumulation
     (the executables apply the same rule)."""
-    if ksplit == 1:
+    if ksplit <= 1:   # whole K, or stream-K (its workspace is a few tens of MB at most)
         return True
     if splits and k > ozaki_kmax(splits):
         return False
@@ -111,7 +121,8 @@ def splitk_applies(m, n, k, ksplit, splits=0):
 def candidates(m=None, n=None, k=None):
     """Every configuration, or those that apply to an m x n x k product."""
     out = [Candidate(t, 0) for t in (TILE_FP64, TILE_FP64_K2, TILE_FP64_K4, TILE_FP64_K8, TILE_FP64_K16,
-                                     TILE_FP64_T64, TILE_FP64_T64_K2, TILE_FP64_T64_K4, TILE_FP64_T64_K8)]
+                                     TILE_FP64_T64, TILE_FP64_T64_K2, TILE_FP64_T64_K4, TILE_FP64_T64_K8,
+                                     TILE_FP64_T64_SK)]
     out += [Candidate(t, s) for t in (TILE_OZAKI_128, TILE_OZAKI_K4, TILE_OZAKI_K16) for s in SPLITS]
     out += [Candidate(TILE_CRT, q) for q in CRT_MODULI]
     if m is not None:

@@ -238,6 +238,9 @@ int mgx_encode_tmap_3d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_byt
 
 // Defined in the kernels' translation units.
 size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit);
+size_t mgx_fp64_streamk_bytes(int m, int n, int k);
+int mgx_launch_dgemm_streamk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                             int ldc, int beta_one, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 int mgx_launch_dgemm_splitk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
                             int ldc, int beta_one, int ksplit, void *partial, size_t partial_bytes,
                             cudaStream_t stream, int tile_m = 128);
@@ -353,6 +356,26 @@ MGX_API int mgx_gemm_fp64_splitk(const double *A, const double *B, double *C, in
     }
     return mgx_launch_dgemm_splitk(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, ksplit, workspace,
                                    workspace_bytes, (cudaStream_t)stream);
+}
+
+MGX_API size_t mgx_fp64_streamk_workspace_size(int m, int n, int k)
+{
+    if (m < 0 || n < 0 || k < 0) return 0;
+    return mgx_fp64_streamk_bytes(m, n, k);
+}
+
+MGX_API int mgx_gemm_fp64_streamk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                                  int ldc, int beta_one, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!dims_ok(m, n, k, lda, ldb, ldc) || (m > 0 && n > 0 && (!C || (k > 0 && (!A || !B))))) {
+        mgx_set_last_message("mgx_gemm_fp64_streamk: invalid arguments m=%d n=%d k=%d lda=%d ldb=%d ldc=%d", m, n, k,
+                             lda, ldb, ldc);
+        return MGX_E_INVALID;
+    }
+    if (m == 0 || n == 0 || k == 0)
+        return mgx_launch_dgemm(A, B, C, m, n, k, 0, k, k, lda, ldb, ldc, beta_one ? 1 : 0, (cudaStream_t)stream, 0);
+    return mgx_launch_dgemm_streamk(A, B, C, m, n, k, lda, ldb, ldc, beta_one ? 1 : 0, workspace, workspace_bytes,
+                                    (cudaStream_t)stream);
 }
 
 MGX_API int mgx_gemm_fp64_tiled(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,

@@ -70,6 +70,10 @@ struct Params {
     const int4 *tiles;  // optional work list (m0, n0, m_end, n_end); null -> regular tiling of m x n
     int num_tiles;
     int panel_kb;       // > 0: add the accumulator into C after every panel_kb K blocks (SUMMA panels)
+    int streamk;        // stream-K (64-row tiles, regular tiling): CTA c takes the K-block units
+                        // [c U / G, (c + 1) U / G) of all U = tiles x kblocks, G = gridDim.x
+    int *sk_tickets;    // stream-K: one arrival counter per tile and consumer warp, zero at launch
+    double *sk_partial; // stream-K: two partial accumulators per CTA (its first and last segment)
     int ksplit;         // > 1: split-K -- work item w is (tile w / ksplit, K slice w % ksplit)
     int kb_split;       // K blocks per slice
     double *partial;    // split-K: slice s of the product goes to partial + s * partial_stride
@@ -132,6 +136,54 @@ __device__ __forceinline__ void item_bounds(const Params &p, int w, int tiles_m,
     kb_end = min(kblocks, kb_begin + p.kb_split);
 }
 
+// The work of one CTA, shared by the producer and the consumers: regular items (tiles or
+// (tile, K slice) pairs, every gridDim.x-th), or in stream-K mode the segments -- pieces of
+// consecutive tiles' K ranges -- of this CTA's contiguous share of all K-block units.
+struct Walk {
+    long long u, u_end;  // stream-K: next unit and the end of this CTA's share
+    int w;               // regular: next work item
+};
+
+__device__ __forceinline__ long long sk_begin(long long c, long long U, long long G) { return c * U / G; }
+
+// CTA whose share holds unit u (sk_begin(c) <= u < sk_begin(c + 1)).
+__device__ __forceinline__ int sk_owner(long long u, long long U, long long G)
+{
+    return (int)(((u + 1) * G + U - 1) / U - 1);
+}
+
+__device__ __forceinline__ void walk_init(const Params &p, int tiles, int kblocks, Walk &s)
+{
+    const long long U = (long long)tiles * kblocks;
+    s.u = sk_begin(blockIdx.x, U, gridDim.x);
+    s.u_end = sk_begin(blockIdx.x + 1, U, gridDim.x);
+    s.w = blockIdx.x;
+    (void)p;
+}
+
+template <int TBM>
+__device__ __forceinline__ bool walk_next(const Params &p, int tiles_m, int tiles_n, int kblocks, int items, Walk &s,
+                                          int &tile, int &m0, int &n0, int &m_end, int &n_end, int &n_lo,
+                                          int &kb_begin, int &kb_end, int &slice)
+{
+    if (p.streamk) {
+        if (s.u >= s.u_end) return false;
+        tile = (int)(s.u / kblocks);
+        kb_begin = (int)(s.u - (long long)tile * kblocks);
+        const long long left = s.u_end - s.u;
+        kb_end = (long long)(kblocks - kb_begin) < left ? kblocks : kb_begin + (int)left;
+        slice = 0;
+        s.u += kb_end - kb_begin;
+        tile_bounds<TBM>(p, tile, tiles_m, tiles_n, m0, n0, m_end, n_end, n_lo);
+        return true;
+    }
+    if (s.w >= items) return false;
+    tile = p.ksplit > 1 ? s.w / p.ksplit : s.w;
+    item_bounds<TBM>(p, s.w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
+    s.w += gridDim.x;
+    return true;
+}
+
 // Swizzled byte offset of element (row, col16) inside a box whose rows are 128 bytes.
 __device__ __forceinline__ uint32_t sw128(int row, int col16)
 {
@@ -182,9 +234,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         int armed_parity[STAGES];
         for (int s = 0; s < STAGES; ++s) armed_parity[s] = -1;
         bool ok = true;
-        for (int w = blockIdx.x; w < items && ok; w += gridDim.x) {
-            int m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
-            item_bounds<TBM>(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
+        Walk walk;
+        walk_init(p, tiles, kblocks, walk);
+        int tile, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
+        while (ok && walk_next<TBM>(p, tiles_m, tiles_n, kblocks, items, walk, tile, m0, n0, m_end, n_end, n_lo,
+                                    kb_begin, kb_end, slice)) {
             for (int kb = kb_begin; kb < kb_end; ++kb) {
                 bool got = true;
                 if (lane == 0) got = mbar_wait_bounded(&empty[stage], phase ^ 1u, p.status, kDevTimeoutEmpty);
@@ -321,9 +375,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     };
 
-    for (int w = blockIdx.x; w < items; w += gridDim.x) {
-        int m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
-        item_bounds<TBM>(p, w, tiles_m, tiles_n, kblocks, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice);
+    Walk walk;
+    walk_init(p, tiles, kblocks, walk);
+    int tile, m0, n0, m_end, n_end, n_lo, kb_begin, kb_end, slice;
+    while (walk_next<TBM>(p, tiles_m, tiles_n, kblocks, items, walk, tile, m0, n0, m_end, n_end, n_lo, kb_begin,
+                          kb_end, slice)) {
 
         double acc[MT][4][4];
 #pragma unroll
@@ -394,7 +450,57 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
         if (!ok) return;
-        if (p.ksplit > 1)
+        if (p.streamk) {
+            if constexpr (TBM == BM_SMALL && !PANELS) {
+                // A tile whose K range spans several CTAs' shares is finished by the CTA that
+                // arrives last at its ticket: every piece's accumulator goes to that CTA's partial
+                // slot, and the last arrival adds the pieces in K order (p0 + p1) + p2 ... and
+                // stores C.  No CTA waits for another.
+                const long long U = (long long)tiles * kblocks, NG = gridDim.x;
+                const long long t0 = (long long)tile * kblocks;
+                const int c0 = sk_owner(t0, U, NG), pieces = sk_owner(t0 + kblocks - 1, U, NG) - c0 + 1;
+                if (pieces == 1) {
+                    store_acc(acc, m0, n0, m_end, n_end, n_lo, p.beta_one, p.C, p.ldc, p.vec_store);
+                } else {
+                    // Each consumer warp owns the same fragment of the tile in every piece, so it
+                    // finishes that fragment on its own: a ticket per (tile, warp), and no barrier
+                    // between the warps (a warp that gave up on a wait cannot block the others).
+                    constexpr int NACC = MT * 16;
+                    constexpr size_t PART = (size_t)CWARPS * 32 * NACC;  // doubles per partial slot
+                    const int ct = threadIdx.x - PRODUCER_WARPS * 32;     // consumer thread 0..255
+                    const int j = (int)blockIdx.x - c0;                    // this CTA's piece
+                    const int slot = (t0 + kb_begin == sk_begin(blockIdx.x, U, NG)) ? 0 : 1;
+                    double(&af)[NACC] = reinterpret_cast<double(&)[NACC]>(acc);
+                    double *mine = p.sk_partial + ((size_t)blockIdx.x * 2 + slot) * PART;
+#pragma unroll
+                    for (int i = 0; i < NACC; ++i) __stcg(mine + (size_t)i * (CWARPS * 32) + ct, af[i]);
+                    __threadfence();
+                    __syncwarp();
+                    int last = 0;
+                    if (lane == 0) last = atomicAdd(p.sk_tickets + (size_t)tile * CWARPS + cw, 1) == pieces - 1;
+                    last = __shfl_sync(0xffffffffu, last, 0);
+                    if (last) {
+                        __threadfence();
+                        double tot[NACC];
+                        const int slot0 = (sk_begin(c0, U, NG) == t0) ? 0 : 1;
+                        const double *p0 = p.sk_partial + ((size_t)c0 * 2 + slot0) * PART;
+#pragma unroll
+                        for (int i = 0; i < NACC; ++i)
+                            tot[i] = j == 0 ? af[i] : __ldcg(p0 + (size_t)i * (CWARPS * 32) + ct);
+                        for (int jj = 1; jj < pieces; ++jj) {
+                            // pieces after the first start their CTA's share: slot 0
+                            const double *pj = p.sk_partial + ((size_t)(c0 + jj) * 2) * PART;
+#pragma unroll
+                            for (int i = 0; i < NACC; ++i)
+                                tot[i] = tot[i] + (jj == j ? af[i] : __ldcg(pj + (size_t)i * (CWARPS * 32) + ct));
+                        }
+#pragma unroll
+                        for (int i = 0; i < NACC; ++i) af[i] = tot[i];
+                        store_acc(acc, m0, n0, m_end, n_end, n_lo, p.beta_one, p.C, p.ldc, p.vec_store);
+                    }
+                }
+            }
+        } else if (p.ksplit > 1)
             store_acc(acc, m0, n0, m_end, n_end, n_lo, 0, p.partial + (size_t)slice * p.partial_stride, p.partial_ld, 1);
         else
             store_acc(acc, m0, n0, m_end, n_end, n_lo, PANELS ? 1 : p.beta_one, p.C, p.ldc, p.vec_store);
@@ -503,7 +609,33 @@ size_t mgx_fp64_splitk_bytes(int m, int n, int k, int ksplit)
 static int launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                         int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
                         const int4 *tiles, int num_tiles, int panel_kb, int ksplit, void *partial,
-                        size_t partial_bytes, int bm = fp64::BM);
+                        size_t partial_bytes, int bm = fp64::BM, int streamk = 0);
+
+// Stream-K workspace: two partial accumulators (256 consumer threads x 32 doubles) per CTA of the
+// grid, then one int ticket per 64 x 128 tile and consumer warp.
+static size_t streamk_partial_bytes(int grid) { return (size_t)grid * 2 * fp64::CWARPS * 32 * 32 * sizeof(double); }
+static int streamk_grid(int m, int n, int k)
+{
+    const long long units = (long long)((m + fp64::BM_SMALL - 1) / fp64::BM_SMALL) * ((n + fp64::BN - 1) / fp64::BN) *
+                            ((k + fp64::BK - 1) / fp64::BK);
+    const int sms = mgx_sm_count();
+    return units < sms ? (int)units : sms;
+}
+
+size_t mgx_fp64_streamk_bytes(int m, int n, int k)
+{
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    const size_t tiles = (size_t)((m + fp64::BM_SMALL - 1) / fp64::BM_SMALL) * ((n + fp64::BN - 1) / fp64::BN);
+    return streamk_partial_bytes(streamk_grid(m, n, k)) + ((tiles * fp64::CWARPS * sizeof(int) + 255) & ~size_t(255));
+}
+
+// Stream-K form over 64 x 128 tiles: every CTA takes an equal share of all tiles' K blocks.
+int mgx_launch_dgemm_streamk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
+                             int ldc, int beta_one, void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    return launch_dgemm(A, B, C, m, n, k, 0, k, k, lda, ldb, ldc, beta_one, stream, 0, nullptr, 0, 0, 1, workspace,
+                        workspace_bytes, fp64::BM_SMALL, 1);
+}
 
 // Launch C (+)= A[:, a_x0 : a_x0 + k_len] * B[0 : k_len, :] with the library's FP64 kernel.
 // a_x_end: A columns at or beyond it read as zero; b_rows: rows of B that exist.
@@ -529,10 +661,15 @@ int mgx_launch_dgemm_splitk(const double *A, const double *B, double *C, int m, 
 static int launch_dgemm(const double *A, const double *B, double *C, int m, int n, int k_len, int a_x0, int a_x_end,
                         int b_rows, int lda, int ldb, int ldc, int beta_one, cudaStream_t stream, int force_generic,
                         const int4 *tiles, int num_tiles, int panel_kb, int ksplit, void *partial,
-                        size_t partial_bytes, int bm)
+                        size_t partial_bytes, int bm, int streamk)
 {
     // SUMMA work lists and panel accumulation are laid out for 128-row tiles
     if (tiles || panel_kb > 0) bm = fp64::BM;
+    // stream-K runs the 64-row tile over a regular tiling only
+    if (streamk && (tiles || panel_kb > 0 || ksplit > 1 || bm != fp64::BM_SMALL)) {
+        mgx_set_last_message("FP64 stream-K: 64-row tiles over a regular tiling only");
+        return MGX_E_INVALID;
+    }
     if (m <= 0 || n <= 0) return MGX_SUCCESS;
     if (k_len <= 0) {
         if (beta_one) return MGX_SUCCESS;
@@ -559,6 +696,9 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
     p.tiles = tiles;
     p.num_tiles = num_tiles;
     p.panel_kb = panel_kb;
+    p.streamk = 0;
+    p.sk_tickets = nullptr;
+    p.sk_partial = nullptr;
     int kb_split = 0, slices = 1;
     splitk_geometry(k_len, (tiles || panel_kb > 0) ? 1 : ksplit, &kb_split, &slices);
     p.ksplit = slices;
@@ -602,7 +742,7 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
         } else {
             rc = launch_dgemm(A2 ? A2 : A, B2 ? B2 : B, C, m, n, k_len, A2 ? 0 : a_x0, A2 ? k_len : a_x_end,
                               B2 ? k_len : b_rows, A2 ? lda2 : lda, B2 ? ldb2 : ldb, ldc, beta_one, stream, 0, tiles,
-                              num_tiles, panel_kb, ksplit, partial, partial_bytes, bm);
+                              num_tiles, panel_kb, ksplit, partial, partial_bytes, bm, streamk);
         }
         cudaFreeAsync(scratch, stream);
         return rc;
@@ -622,6 +762,20 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
     const int total_items = tiles_list_or(tiles, num_tiles, m, n, bm) * slices;
     int grid = mgx_sm_count();
     if (grid > total_items) grid = total_items;
+    if (streamk) {
+        grid = streamk_grid(m, n, k_len);
+        const size_t pbytes = streamk_partial_bytes(grid);
+        const size_t ntickets = (size_t)total_items * fp64::CWARPS;
+        if (!partial || partial_bytes < pbytes + ntickets * sizeof(int) || (reinterpret_cast<uintptr_t>(partial) & 255)) {
+            mgx_set_last_message("FP64 stream-K: workspace of %zu bytes (aligned to 256) needed, %zu given",
+                                 pbytes + ntickets * sizeof(int), partial_bytes);
+            return MGX_E_WORKSPACE;
+        }
+        p.streamk = 1;
+        p.sk_partial = reinterpret_cast<double *>(partial);
+        p.sk_tickets = reinterpret_cast<int *>(reinterpret_cast<char *>(partial) + pbytes);
+        MGX_HOST_CHECK(cudaMemsetAsync(p.sk_tickets, 0, ntickets * sizeof(int), stream));
+    }
     auto launch = [&](auto kernel, int smem_bytes) -> int {
         cudaFuncAttributes fa;
         MGX_HOST_CHECK(cudaFuncGetAttributes(&fa, kernel));

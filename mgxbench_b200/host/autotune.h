@@ -83,8 +83,9 @@ inline std::string default_model_path() { return exe_dir() + "/../mgxbench_b200/
 
 // Tile ids of the candidates (mgxbench_b200.autotune): 0, 2, 3, 4, 5 are the FP64 kernel's
 // 128 x 128 tiles with the K range cut into 1, 2, 4, 8, 16 slices; 9, 10, 11, 12 its 64 x 128
-// tiles with 1, 2, 4, 8 slices; 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices; 8 is the CRT
-// form (its "splits" is the modulus count).
+// tiles with 1, 2, 4, 8 slices and 13 its 64 x 128 tiles in the stream-K schedule (K slices 0);
+// 1, 6, 7 are the Ozaki kernel with 1, 4, 16 slices; 8 is the CRT form (its "splits" is the
+// modulus count).
 inline int tile_ksplit(int tile)
 {
     switch (tile) {
@@ -97,11 +98,12 @@ inline int tile_ksplit(int tile)
     case 10: return 2;
     case 11: return 4;
     case 12: return 8;
+    case 13: return 0;  // stream-K
     default: return 1;
     }
 }
 
-inline int tile_rows(int tile) { return (tile >= 9 && tile <= 12) ? 64 : 128; }
+inline int tile_rows(int tile) { return (tile >= 9 && tile <= 13) ? 64 : 128; }
 inline bool tile_is_crt(int tile) { return tile == 8; }
 inline bool tile_is_fp64(int tile) { return tile != 1 && tile != 6 && tile != 7 && !tile_is_crt(tile); }
 
@@ -109,7 +111,7 @@ inline bool tile_is_fp64(int tile) { return tile != 1 && tile != 6 && tile != 7 
 // partial products fit 4 GiB, and an Ozaki split needs K within one int32 accumulation.
 inline bool splitk_applies(int m, int n, int k, int ksplit, int splits)
 {
-    if (ksplit == 1) return true;
+    if (ksplit <= 1) return true;  // whole K, or stream-K
     if (splits > 0 && k > mgx_ozaki_kmax(splits)) return false;
     return (k + 31) / 32 >= ksplit && (double)ksplit * m * n * 8.0 <= 4294967296.0;
 }
@@ -140,9 +142,9 @@ inline int auto_choose(const std::string &path, int m, int n, int k, double exp_
         return -1;
     }
     if (!json_numbers(text, "candidates", &cand) || cand.empty() || cand.size() % 2) {
-        // default list: FP64 128-row tiles (1..16 K slices) and 64-row tiles (1..8), Ozaki 3..9
+        // default list: FP64 128-row tiles (1..16 K slices) and 64-row tiles (1..8, stream-K), Ozaki 3..9
         // splits with 1, 4, 16 K slices, CRT 9, 11..16 moduli
-        cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0, 9, 0, 10, 0, 11, 0, 12, 0};
+        cand = {0, 0, 2, 0, 3, 0, 4, 0, 5, 0, 9, 0, 10, 0, 11, 0, 12, 0, 13, 0};
         for (int t : {1, 6, 7})
             for (int s = 3; s <= 9; ++s) {
                 cand.push_back(t);

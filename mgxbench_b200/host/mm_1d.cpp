@@ -96,6 +96,8 @@ int main(int argc, char *argv[])
         splits = mm::env_int("MGXBENCH_MODULI", mgx_crt_choose_moduli(chunked ? std::min(pipeline_k_chunk, k) : k, 1e-15));
     if (form == mm::kCrt) ksplit = 1;
     if (form != mm::kFp64 || chunked) tile_m = 128;  // the 64-row tile is an FP64 whole-multiply option
+    if (ksplit < 0 || (ksplit == 0 && form != mm::kFp64)) ksplit = 1;  // 0: FP64 stream-K (64-row tiles)
+    if (ksplit == 0) tile_m = 64;
     const int graph = mm::env_int("MGXBENCH_GRAPH", 0);
     printf("mmb one-GPU emulation: ranks=%d rows/rank=%d form=%s%s input=%s B-structure=%s", nRanks, mi,
            form_name.c_str(), mm::form_count(form, splits).c_str(), input_name.c_str(), chunked ? "K-chunked" : "single");
@@ -223,6 +225,7 @@ int main(int argc, char *argv[])
            input_name.c_str());
     printf("%s", mm::form_count(form, splits).c_str());
     if (ksplit > 1) printf(" ksplit=%d", ksplit);
+    if (ksplit == 0) printf(" streamk=1");
     if (tile_m != 128) printf(" tile_m=%d", tile_m);
     if (input != mm::kConst) printf(" norm_rel_err=%.3e max_rel_err=%.3e", err.normwise, err.max_rel);
     printf("\n");

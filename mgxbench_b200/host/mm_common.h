@@ -126,11 +126,18 @@ struct Workspace {
     }
 };
 
-// One block multiply C (+)= A B of the selected form with `ksplit` K slices (`splits` holds the
-// modulus count for the CRT form; tile_m the FP64 output tile height, 64 or 128).
+// One block multiply C (+)= A B of the selected form with `ksplit` K slices (0: the FP64
+// stream-K schedule; `splits` holds the modulus count for the CRT form; tile_m the FP64 output
+// tile height, 64 or 128).
 inline int block_gemm(int form, int splits, int ksplit, Workspace &ws, const double *A, const double *B, double *C,
                       int m, int n, int k, int lda, int ldb, int ldc, int beta_one, cudaStream_t s, int tile_m = 128)
 {
+    if (form == kFp64 && ksplit == 0) {  // stream-K over 64 x 128 tiles
+        const size_t need = mgx_fp64_streamk_workspace_size(m, n, k);
+        void *w = ws.get(need);
+        if (!w && need) return MGX_E_CUDA;
+        return mgx_gemm_fp64_streamk(A, B, C, m, n, k, lda, ldb, ldc, beta_one, w, need, s);
+    }
     if (form == kFp64 && tile_m != 128) {
         const size_t need = ksplit > 1 ? mgx_fp64_splitk_workspace_size(m, n, k, ksplit) : 0;
         void *w = need ? ws.get(need) : nullptr;

@@ -19,8 +19,9 @@ def synthetic_rows(shapes, seed=0):
             if c.is_fp64:
                 # split-K and the 64-row tile help only products with few output tiles
                 tiles = math.ceil(m / c.tile_m) * math.ceil(n / 128)
-                t = f / 30e12 * max(1.0, 148 / tiles) / min(c.ksplit, max(1.0, 148 / tiles)) + 3e-6 * c.ksplit
-                e = 1e-15 * math.sqrt(k / 1e3 / c.ksplit)
+                ks = c.ksplit if c.ksplit else 148 / tiles   # stream-K fills every SM
+                t = f / 30e12 * max(1.0, 148 / tiles) / min(ks, max(1.0, 148 / tiles)) + 3e-6 * max(ks, 1)
+                e = 1e-15 * math.sqrt(k / 1e3 / max(ks, 1))
             elif c.is_crt:
                 L = sum(math.log2(p) for p in (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211,
                                                199, 197, 193)[:c.splits])
@@ -40,22 +41,24 @@ def test_candidates_and_features():
     assert cs[0].tile == at.TILE_FP64 and cs[0].splits == 0 and cs[0].ksplit == 1
     assert [c.ksplit for c in cs if c.is_fp64 and c.tile_m == 128] == [1, 2, 4, 8, 16]
     # the second FP64 tile shape (64 x 128) is a candidate of its own, with its own tile id
-    assert [(c.tile, c.ksplit) for c in cs if c.is_fp64 and c.tile_m == 64] == [(9, 1), (10, 2), (11, 4), (12, 8)]
+    assert [(c.tile, c.ksplit) for c in cs if c.is_fp64 and c.tile_m == 64] == [(9, 1), (10, 2), (11, 4), (12, 8),
+                                                                                (13, 0)]
+    assert next(c for c in cs if c.tile == 13).name == "fp64t64sk"
     assert {c.tile_m for c in cs if not c.is_fp64} == {128}
     assert [c.splits for c in cs if c.form == "ozaki" and c.ksplit == 1] == list(range(3, 10))
     assert sorted({c.ksplit for c in cs if c.form == "ozaki"}) == [1, 4, 16]
     assert [c.splits for c in cs if c.is_crt] == list(at.CRT_MODULI) and {c.ksplit for c in cs if c.is_crt} == {1}
-    assert len({c.name for c in cs}) == len(cs) == 5 + 4 + 3 * 7 + 7
+    assert len({c.name for c in cs}) == len(cs) == 5 + 5 + 3 * 7 + 7
     oz5 = next(c for c in cs if c.splits == 5)
     f = at.features(1024, 2048, 4096, 20, oz5)
     assert f[:3] == [10.0, 11.0, 12.0] and f[3:] == [20.0, 1.0, 5.0]
     # split-K candidates only where the K range has the blocks and the slices fit the workspace cap
     small = at.candidates(300, 300, 100)            # 4 K blocks
     assert [c.ksplit for c in small if c.is_fp64 and c.tile_m == 128] == [1, 2, 4]
-    assert [c.ksplit for c in small if c.is_fp64 and c.tile_m == 64] == [1, 2, 4]
+    assert [c.ksplit for c in small if c.is_fp64 and c.tile_m == 64] == [1, 2, 4, 0]
     assert sorted({c.ksplit for c in small if c.form == "ozaki"}) == [1, 4]
     big = at.candidates(32768, 32768, 32768)
-    assert [c.ksplit for c in big if c.is_fp64] == [1, 1] and {c.ksplit for c in big} == {1}
+    assert [c.ksplit for c in big if c.is_fp64] == [1, 1, 0] and {c.ksplit for c in big} == {0, 1}
     # an Ozaki K slice needs K within one int32 accumulation
     assert at.ozaki_kmax(9) == 58240 and not at.splitk_applies(64, 64, 60000, 4, 9)
     assert at.splitk_applies(64, 64, 60000, 4, 8)

@@ -249,3 +249,39 @@ def test_small_tile_beta_one_and_odd_pitch(mgx, oracle):
     assert torch.equal(c64.view(torch.int64), c128.view(torch.int64))
     ref = C0 + oracle.ab_multiply(np.ascontiguousarray(A), np.ascontiguousarray(B))
     assert np.all(np.abs(host(c64) - ref) <= 2 * gamma(k + 1) * (np.abs(A) @ np.abs(B) + np.abs(C0)))
+
+
+@pytest.mark.parametrize("m,n,k", [(1024, 1024, 1024), (64, 128, 32), (64, 128, 4096), (333, 127, 1000),
+                                   (2200, 300, 200), (100, 700, 5000), (1, 1, 1), (4096, 2048, 512)])
+def test_streamk_within_bound_and_deterministic(mgx, oracle, m, n, k):
+    """Stream-K over 64 x 128 tiles (mgx_gemm_fp64_streamk): every CTA takes an equal share of all
+    tiles' K blocks, and a tile split between CTAs is finished by the last to arrive, adding the
+    pieces in K order.  Shapes with one unit per CTA, a single tile split into 128 pieces, and
+    tiles split at uneven places; the result is inside the oracle's bound and identical on a
+    second run."""
+    import torch
+    rng = np.random.default_rng(m * 5 + n + k)
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    dA, dB = dev(A), dev(B)
+    c1 = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    c2 = torch.full((m, n), np.nan, dtype=torch.float64, device="cuda")
+    mgx.gemm_fp64(dA, dB, c1, ksplit=0)
+    mgx.gemm_fp64(dA, dB, c2, ksplit=0)
+    assert torch.equal(c1.view(torch.int64), c2.view(torch.int64))
+    check_close(host(c1), A, B, oracle, k)
+    assert mgx.device_status() == 0
+
+
+def test_streamk_beta_one_and_odd_pitch(mgx, oracle):
+    import torch
+    rng = np.random.default_rng(8)
+    m, n, k = 150, 100, 1300
+    Ab, Bb = rng_matrix(rng, (m, k + 1)), rng_matrix(rng, (k, n + 1))
+    A, B = Ab[:, :k], Bb[:, :n]
+    C0 = rng_matrix(rng, (m, n))
+    dAb, dBb = dev(Ab), dev(Bb)
+    dC = dev(C0)
+    mgx.gemm_fp64(dAb[:, :k], dBb[:, :n], dC, beta_one=True, ksplit=0)
+    ref = C0 + oracle.ab_multiply(np.ascontiguousarray(A), np.ascontiguousarray(B))
+    assert np.all(np.abs(host(dC) - ref) <= 2 * gamma(k + 1) * (np.abs(A) @ np.abs(B) + np.abs(C0)))
+    assert mgx.device_status() == 0

@@ -19,7 +19,7 @@ def _synthetic_db(path):
         for c in at.candidates():
             mnk = float(d) ** 3
             if c.is_fp64:
-                t, e = 2 * mnk / 35e12 / min(c.ksplit, 4) ** (0.5 if d < 1024 else 0.0) + 2e-5, 3e-16
+                t, e = 2 * mnk / 35e12 / min(c.ksplit or 4, 4) ** (0.5 if d < 1024 else 0.0) + 2e-5, 3e-16
             else:
                 t, e = c.splits * (c.splits + 1) / 2 * 2 * mnk / 3e15 + 1e-4, 10.0 ** (-8 - 2 * (c.splits - 3)) * 3
             rows.append({"m": d, "n": d, "k": d, "exp_range": 10, "tile": c.tile, "splits": c.splits,
