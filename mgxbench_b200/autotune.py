@@ -176,6 +176,11 @@ def measure(m, n, k, exp_range, cands, seed=0, check_rows=32, reps=None):
         out.append({"m": m, "n": n, "k": k, "exp_range": exp_range, "tile": c.tile, "splits": c.splits,
                     "seconds": t, "tflops": flop / t / 1e12, "error": max(errors[key], ERROR_FLOOR)})
     del A, B, C, ws
+    # hand back the cached device memory (torch's and the library's scratch pool) so that a sweep
+    # over hundreds of shapes up to 32768 does not accumulate it
+    torch.cuda.synchronize()
+    mgx.scratch_trim()
+    torch.cuda.empty_cache()
     return out
 
 
