@@ -41,7 +41,10 @@ CHECK_ROWS = 256
 # DRAM bytes (read + write) per launch of the dominant kernel at N = 16384, from one-pass ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum) of bench.py at full size:
 # ozaki_gemm with s = 8 reads 83.69 GB and writes 2.15 GB; crt_gemm with q = 15 reads
-# 48.43 GB and writes 4.03 GB.
+# 48.43 GB and writes 4.03 GB.  (Counter captures now run at N = 8192, where crt_gemm moves
+# 5.41 GB, 1.79x its algorithmic bytes; scaled by the algorithmic bytes that would be 21.7 GB
+# at N = 16384, an underestimate because a modulus's operands outgrow L2, so the measured
+# full-size figure is kept.)
 OZAKI_GEMM_TRAFFIC_BYTES = 85.84e9
 CRT_GEMM_TRAFFIC_BYTES = 52.46e9
 

@@ -56,7 +56,7 @@ CRT_KMAX = 130816
 # A CRT candidate must predict an error this many times below the target: its error falls only
 # ~10x per added modulus and grows with sqrt(K), so predictions near a target need a guard band
 # (the slice form's falls ~100x per slice).  The band covers the measured / predicted error
-# ratio of the CRT runs in the training set (99th percentile 1.81, maximum 2.04 on the packaged
+# ratio of the CRT runs in the training set (99th percentile 1.72, maximum 1.87 on the packaged
 # sweep).  Same constant in host/autotune.h.
 CRT_ERROR_MARGIN = 2.0
 ERROR_FLOOR = 1e-17
