@@ -471,14 +471,24 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const int j = (int)blockIdx.x - c0;                    // this CTA's piece
                     const int slot = (t0 + kb_begin == sk_begin(blockIdx.x, U, NG)) ? 0 : 1;
                     double(&af)[NACC] = reinterpret_cast<double(&)[NACC]>(acc);
-                    double *mine = p.sk_partial + ((size_t)blockIdx.x * 2 + slot) * PART;
-#pragma unroll
-                    for (int i = 0; i < NACC; ++i) __stcg(mine + (size_t)i * (CWARPS * 32) + ct, af[i]);
-                    __threadfence();
-                    __syncwarp();
+                    int *ticket = p.sk_tickets + (size_t)tile * CWARPS + cw;
+                    // The head piece is usually computed last (at the end of its CTA's share):
+                    // when every later piece has taken its ticket, it finishes the tile without
+                    // writing its own partial.
                     int last = 0;
-                    if (lane == 0) last = atomicAdd(p.sk_tickets + (size_t)tile * CWARPS + cw, 1) == pieces - 1;
-                    last = __shfl_sync(0xffffffffu, last, 0);
+                    if (j == 0) {
+                        if (lane == 0) last = atomicAdd(ticket, 0) == pieces - 1;
+                        last = __shfl_sync(0xffffffffu, last, 0);
+                    }
+                    if (!last) {
+                        double *mine = p.sk_partial + ((size_t)blockIdx.x * 2 + slot) * PART;
+#pragma unroll
+                        for (int i = 0; i < NACC; ++i) __stcg(mine + (size_t)i * (CWARPS * 32) + ct, af[i]);
+                        __threadfence();
+                        __syncwarp();
+                        if (lane == 0) last = atomicAdd(ticket, 1) == pieces - 1;
+                        last = __shfl_sync(0xffffffffu, last, 0);
+                    }
                     if (last) {
                         __threadfence();
                         double tot[NACC];
