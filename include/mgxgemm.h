@@ -133,7 +133,8 @@ MGX_API int mgx_gemm_fp64_tiled(const double *A, const double *B, double *C, int
  * split between CTAs is finished by the last of them to arrive, which adds the pieces in K order.
  * No CTA waits for another.  Deterministic for a given GPU (the shares depend on its SM count),
  * and within the same any-order bound as the other FP64 entry points.  `workspace` (256-byte
- * aligned) holds mgx_fp64_streamk_workspace_size(m, n, k) bytes on the current device. */
+ * aligned) holds mgx_fp64_streamk_workspace_size(m, n, k) bytes on the current device; its
+ * contents need no initialisation (the arrival tickets carry a per-launch tag). */
 MGX_API size_t mgx_fp64_streamk_workspace_size(int m, int n, int k);
 MGX_API int mgx_gemm_fp64_streamk(const double *A, const double *B, double *C, int m, int n, int k, int lda, int ldb,
                                   int ldc, int beta_one, void *workspace, size_t workspace_bytes, void *stream);

@@ -16,6 +16,7 @@
 // Operands TMA cannot describe (odd leading dimension, odd K offset, unaligned base) are first
 // copied into stream-ordered scratch with an even pitch.  A variant whose producer warp loads
 // with plain global loads covers the one case with nothing to copy (a chunk wholly past k_total).
+#include <atomic>
 #include <cstdio>
 
 #include "mgx_common.cuh"
@@ -72,7 +73,8 @@ struct Params {
     int panel_kb;       // > 0: add the accumulator into C after every panel_kb K blocks (SUMMA panels)
     int streamk;        // stream-K (64-row tiles, regular tiling): CTA c takes the K-block units
                         // [c U / G, (c + 1) U / G) of all U = tiles x kblocks, G = gridDim.x
-    int *sk_tickets;    // stream-K: one arrival counter per tile and consumer warp, zero at launch
+    unsigned long long *sk_tickets;  // stream-K: one arrival ticket per tile and consumer warp
+    unsigned long long sk_epoch;     // stream-K: this launch's ticket tag (a ticket of another tag counts 0)
     double *sk_partial; // stream-K: two partial accumulators per CTA (its first and last segment)
     int ksplit;         // > 1: split-K -- work item w is (tile w / ksplit, K slice w % ksplit)
     int kb_split;       // K blocks per slice
@@ -190,6 +192,30 @@ __device__ __forceinline__ uint32_t sw128(int row, int col16)
     return row * 128 + ((((col16 >> 1) ^ (row & 7)) & 7) << 4) + ((col16 & 1) << 3);
 }
 
+// Stream-K tickets: (launch tag << 8) | arrivals.  A ticket written by an earlier launch (another
+// tag), or never written, counts as no arrivals, so the tickets need no reset between launches.
+// Arrivals per tile are at most the grid size, below 256.
+__device__ __forceinline__ int ticket_count(unsigned long long *tk, unsigned long long tag)
+{
+    const unsigned long long v = atomicAdd(tk, 0ull);
+    return (v >> 8) == tag ? (int)(v & 255u) : 0;
+}
+
+// Takes a ticket; returns the arrivals before this one, or -1 (status set) if the compare-and-swap
+// never got through (each failure is another arrival's success, so this does not happen).
+__device__ __forceinline__ int ticket_take(unsigned long long *tk, unsigned long long tag, int *status)
+{
+    unsigned long long old = atomicAdd(tk, 0ull);
+    for (int it = 0; it < 4096; ++it) {
+        const unsigned long long cur = (old >> 8) == tag ? old : (tag << 8);
+        const unsigned long long prev = atomicCAS(tk, old, cur + 1);
+        if (prev == old) return (int)(cur & 255u);
+        old = prev;
+    }
+    record_status(status, kDevTicket);
+    return -1;
+}
+
 template <int TBM, bool USE_TMA, bool PANELS>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
@@ -218,6 +244,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         tma_prefetch_desc(&tmB);
     }
     __syncthreads();
+    // Launched as a programmatic dependent: everything above overlapped the previous kernel in the
+    // stream; nothing below reads or writes memory before that kernel has finished.  The next
+    // kernel may be scheduled now (it cannot share an SM with this one, and waits the same way).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
     const int tiles_m = (p.m + TBM - 1) / TBM;
     const int tiles_n = (p.n + BN - 1) / BN;
@@ -471,13 +502,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const int j = (int)blockIdx.x - c0;                    // this CTA's piece
                     const int slot = (t0 + kb_begin == sk_begin(blockIdx.x, U, NG)) ? 0 : 1;
                     double(&af)[NACC] = reinterpret_cast<double(&)[NACC]>(acc);
-                    int *ticket = p.sk_tickets + (size_t)tile * CWARPS + cw;
+                    unsigned long long *ticket = p.sk_tickets + (size_t)tile * CWARPS + cw;
                     // The head piece is usually computed last (at the end of its CTA's share):
                     // when every later piece has taken its ticket, it finishes the tile without
                     // writing its own partial.
                     int last = 0;
                     if (j == 0) {
-                        if (lane == 0) last = atomicAdd(ticket, 0) == pieces - 1;
+                        if (lane == 0) last = ticket_count(ticket, p.sk_epoch) == pieces - 1;
                         last = __shfl_sync(0xffffffffu, last, 0);
                     }
                     if (!last) {
@@ -486,7 +517,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         for (int i = 0; i < NACC; ++i) __stcg(mine + (size_t)i * (CWARPS * 32) + ct, af[i]);
                         __threadfence();
                         __syncwarp();
-                        if (lane == 0) last = atomicAdd(ticket, 1) == pieces - 1;
+                        if (lane == 0) last = ticket_take(ticket, p.sk_epoch, p.status) == pieces - 1;
                         last = __shfl_sync(0xffffffffu, last, 0);
                     }
                     if (last) {
@@ -622,7 +653,7 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
                         size_t partial_bytes, int bm = fp64::BM, int streamk = 0);
 
 // Stream-K workspace: two partial accumulators (256 consumer threads x 32 doubles) per CTA of the
-// grid, then one int ticket per 64 x 128 tile and consumer warp.
+// grid, then one 8-byte ticket per 64 x 128 tile and consumer warp.
 static size_t streamk_partial_bytes(int grid) { return (size_t)grid * 2 * fp64::CWARPS * 32 * 32 * sizeof(double); }
 static int streamk_grid(int m, int n, int k)
 {
@@ -636,7 +667,8 @@ size_t mgx_fp64_streamk_bytes(int m, int n, int k)
 {
     if (m <= 0 || n <= 0 || k <= 0) return 0;
     const size_t tiles = (size_t)((m + fp64::BM_SMALL - 1) / fp64::BM_SMALL) * ((n + fp64::BN - 1) / fp64::BN);
-    return streamk_partial_bytes(streamk_grid(m, n, k)) + ((tiles * fp64::CWARPS * sizeof(int) + 255) & ~size_t(255));
+    return streamk_partial_bytes(streamk_grid(m, n, k)) +
+           ((tiles * fp64::CWARPS * sizeof(unsigned long long) + 255) & ~size_t(255));
 }
 
 // Stream-K form over 64 x 128 tiles: every CTA takes an equal share of all tiles' K blocks.
@@ -774,17 +806,24 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
     if (grid > total_items) grid = total_items;
     if (streamk) {
         grid = streamk_grid(m, n, k_len);
+        if (grid > 255) {  // arrivals per tile must fit a ticket's 8-bit count
+            mgx_set_last_message("FP64 stream-K: grid of %d CTAs exceeds 255", grid);
+            return MGX_E_UNSUPPORTED;
+        }
         const size_t pbytes = streamk_partial_bytes(grid);
         const size_t ntickets = (size_t)total_items * fp64::CWARPS;
-        if (!partial || partial_bytes < pbytes + ntickets * sizeof(int) || (reinterpret_cast<uintptr_t>(partial) & 255)) {
+        const size_t tbytes = ntickets * sizeof(unsigned long long);
+        if (!partial || partial_bytes < pbytes + tbytes || (reinterpret_cast<uintptr_t>(partial) & 255)) {
             mgx_set_last_message("FP64 stream-K: workspace of %zu bytes (aligned to 256) needed, %zu given",
-                                 pbytes + ntickets * sizeof(int), partial_bytes);
+                                 pbytes + tbytes, partial_bytes);
             return MGX_E_WORKSPACE;
         }
         p.streamk = 1;
         p.sk_partial = reinterpret_cast<double *>(partial);
-        p.sk_tickets = reinterpret_cast<int *>(reinterpret_cast<char *>(partial) + pbytes);
-        MGX_HOST_CHECK(cudaMemsetAsync(p.sk_tickets, 0, ntickets * sizeof(int), stream));
+        p.sk_tickets = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(partial) + pbytes);
+        // a fresh tag per launch (56 bits, never 0: zeroed memory reads as no arrivals)
+        static std::atomic<unsigned long long> epochs{0};
+        p.sk_epoch = ((epochs.fetch_add(1, std::memory_order_relaxed) + 1) & ((1ull << 56) - 1));
     }
     auto launch = [&](auto kernel, int smem_bytes) -> int {
         cudaFuncAttributes fa;
@@ -795,7 +834,20 @@ static int launch_dgemm(const double *A, const double *B, double *C, int m, int 
             return MGX_E_UNSUPPORTED;
         }
         MGX_HOST_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
-        kernel<<<grid, fp64::THREADS, smem_bytes, stream>>>(tmA, tmB, p);
+        // programmatic dependent launch: the set-up above griddepcontrol.wait overlaps the end of
+        // the previous kernel in the stream
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof cfg);
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(fp64::THREADS);
+        cfg.dynamicSmemBytes = (size_t)smem_bytes;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        MGX_HOST_CHECK(cudaLaunchKernelEx(&cfg, kernel, tmA, tmB, p));
         return MGX_SUCCESS;
     };
     constexpr int S128 = fp64::Geo<fp64::BM>::SMEM_BYTES, S64 = fp64::Geo<fp64::BM_SMALL>::SMEM_BYTES;

@@ -47,6 +47,7 @@ enum DeviceStatus : int {
     kDevTimeoutAcc = 3,      // accumulator hand-off wait ran out
     kDevNonFinite = 4,       // non-finite input where the form cannot represent it
     kDevBadLaunch = 5,       // launch geometry does not match the kernel's assumptions
+    kDevTicket = 6,          // a stream-K ticket could not be taken
 };
 
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait

@@ -272,6 +272,38 @@ def test_streamk_within_bound_and_deterministic(mgx, oracle, m, n, k):
     assert mgx.device_status() == 0
 
 
+def test_streamk_tickets_need_no_reset(mgx, oracle):
+    """The stream-K tickets are tagged per launch instead of being cleared before it: a workspace
+    full of arbitrary bytes, and one left by a product of another tiling (tickets of other tiles
+    at other counts), give the same bits as a fresh zeroed workspace."""
+    import torch
+    rng = np.random.default_rng(77)
+    m, n, k = 1024, 1024, 1024
+    A, B = rng_matrix(rng, (m, k), "wide"), rng_matrix(rng, (k, n), "wide")
+    dA, dB = dev(A), dev(B)
+    need = mgx.lib().mgx_fp64_streamk_workspace_size(m, n, k)
+    fresh = mgx.OzakiWorkspace()
+    fresh.get(need).zero_()
+    ref = torch.empty((m, n), dtype=torch.float64, device="cuda")
+    mgx.gemm_fp64(dA, dB, ref, ksplit=0, workspace=fresh)
+    junk = mgx.OzakiWorkspace()
+    buf = junk.get(need)
+    buf.copy_(torch.from_numpy(rng.integers(0, 256, buf.numel(), dtype=np.uint8)).cuda())
+    c = torch.empty_like(ref)
+    mgx.gemm_fp64(dA, dB, c, ksplit=0, workspace=junk)
+    assert torch.equal(c.view(torch.int64), ref.view(torch.int64))
+    # another tiling on the same workspace first, then this product again, twice in a row
+    A2, B2 = rng_matrix(rng, (333, 5000), "wide"), rng_matrix(rng, (5000, 700), "wide")
+    c2 = torch.empty((333, 700), dtype=torch.float64, device="cuda")
+    mgx.gemm_fp64(dev(A2), dev(B2), c2, ksplit=0, workspace=junk)
+    for _ in range(2):
+        c.fill_(np.nan)
+        mgx.gemm_fp64(dA, dB, c, ksplit=0, workspace=junk)
+        assert torch.equal(c.view(torch.int64), ref.view(torch.int64))
+    check_close(host(ref), A, B, oracle, k)
+    assert mgx.device_status() == 0
+
+
 def test_streamk_beta_one_and_odd_pitch(mgx, oracle):
     import torch
     rng = np.random.default_rng(8)
