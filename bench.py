@@ -142,6 +142,18 @@ def ranks_reduce_max(dist, value: float, device) -> float:
     return float(t.item())
 
 
+def host_cpu_model() -> str:
+    """The host CPU's model name (from /proc/cpuinfo), for the CPU baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
@@ -170,7 +182,8 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"dgemm_n{n}_wide_exp{EXP_RANGE}", "m": n, "n": n, "k": n,
                    "form": "reference FP64 FMA chain on host cores", "sample_rows": rows},
-        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": host_cpu_model(), "host_cpus": os.cpu_count()},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -393,7 +406,7 @@ def run_ours(args):
             dt = time.perf_counter() - t0
             cpu = {"value": 2.0 * rows * n * n / dt / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                    "sample": f"{rows} rows x {n} x {n} of the N={n} product (oracle FMA-chain restatement of "
-                             f"sharedABMultiply), {dt:.1f} s"}
+                             f"sharedABMultiply), {dt:.1f} s", "cpu_model": host_cpu_model(), "host_cpus": os.cpu_count()}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "TFLOP/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
 
