@@ -63,17 +63,45 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock, power and clock-event (throttle) reasons sampled during a timed region: through
+    NVML every 10 ms where the binding is present, else nvidia-smi every 200 ms.  It only reads."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+    PERIOD_S = 0.01
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, uuid: str | None = None):
         self.dev = device_index
+        self.uuid = uuid
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, power W, reason bits)
+        self.done = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        if self.uuid:
+            for u in (self.uuid if self.uuid.startswith("GPU-") else "GPU-" + self.uuid, self.uuid):
+                try:
+                    return pynvml, pynvml.nvmlDeviceGetHandleByUUID(u)
+                except Exception:
+                    pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.nvml = (nv, h)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
@@ -83,11 +111,31 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml
+        while not self.done.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                     nv.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                                     int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+            except Exception:
+                pass
+            self.done.wait(self.PERIOD_S)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml:
+            self.done.set()
+            self.thread.join(timeout=2)
+            sms = [x[0] for x in self.samples]
+            power = [x[1] for x in self.samples]
+            reasons = {name for name, bit in self.REASONS for x in self.samples if x[2] & bit}
+            return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": self.max_mhz,
+                    "power_w_max": max(power) if power else None, "samples": len(sms),
+                    "source": f"NVML every {self.PERIOD_S * 1000:.0f} ms", "reasons": sorted(reasons)}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -97,7 +145,7 @@ class ClockSampler:
             self.proc.kill()
         self.thread.join(timeout=2)
         sms, maxes, power, reasons = [], [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        names = [name for name, _ in self.REASONS]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
@@ -112,7 +160,16 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
-                "power_w_max": max(power) if power else None, "samples": len(sms), "reasons": sorted(reasons)}
+                "power_w_max": max(power) if power else None, "samples": len(sms),
+                "source": "nvidia-smi every 200 ms", "reasons": sorted(reasons)}
+
+
+def device_uuid(torch) -> str | None:
+    """The current CUDA device's UUID (NVML names the same GPU by it whatever CUDA_VISIBLE_DEVICES is)."""
+    try:
+        return str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        return None
 
 
 def cpu_reference_rate(n: int, budget_s: float, threads: int = 0):
@@ -243,7 +300,8 @@ def run_ours(args):
         step()
     stream.synchronize()
 
-    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank)
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank,
+                           device_uuid(torch))
     sampler.start()
     time.sleep(0.3)
     barrier()
@@ -362,7 +420,8 @@ def run_ours(args):
     # a short burst before the timed region, and a sustained figure -- one launch of about
     # 2.5 s, long enough for the 1 kW power cap to set the clock -- after it.  ozaki_gemm runs
     # ~100 ms launches back to back inside a long step, so the sustained figure is its ceiling.
-    peak_sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank)
+    peak_sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank,
+                                device_uuid(torch))
     peak_sampler.start()
     time.sleep(0.3)
     int8_sustained = mgx.peak_int8(1, 60_000_000)
