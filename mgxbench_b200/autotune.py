@@ -443,10 +443,47 @@ def run_sweep(db_path, train_shapes=2000, heldout_shapes=500, seed=0, budget_s=N
     return db
 
 
+def refresh_rows(db_path, tiles, seed=0, train_shapes=2000, heldout_shapes=500, budget_s=None, log=print):
+    """Measures again the database rows of the given tile ids (after a change to those kernels),
+    with the inputs the sweep used for each shape, and rewrites the database.  Resumable: a row
+    already refreshed carries "refreshed": the tag, and a run that reaches the budget writes what
+    it has."""
+    db = SweepDB(db_path)
+    tiles = set(tiles)
+    tag = "tiles " + ",".join(str(t) for t in sorted(tiles))
+    train = [s for s in random_shapes(train_shapes * 2, seed + 1) if shape_fits(*s[:3])][:train_shapes]
+    held = [s for s in random_shapes(heldout_shapes * 2, seed + 2) if shape_fits(*s[:3])][:heldout_shapes]
+    seeds = {("train", s): i for i, s in enumerate(train)}
+    seeds.update({("heldout", s): 100000 + i for i, s in enumerate(held)})
+    groups = {}
+    for idx, r in enumerate(db.rows):
+        if r["tile"] in tiles and r.get("refreshed") != tag:
+            groups.setdefault((r.get("set"), (r["m"], r["n"], r["k"], r["exp_range"])), []).append(idx)
+    t0 = time.time()
+    done = 0
+    for (which, shape), idxs in groups.items():
+        if (which, shape) not in seeds:
+            continue
+        cands = [Candidate(db.rows[i]["tile"], db.rows[i]["splits"]) for i in idxs]
+        for i, new in zip(idxs, measure(*shape, cands, seed=seeds[(which, shape)])):
+            new["set"] = which
+            new["refreshed"] = tag
+            db.rows[i] = new
+        done += 1
+        if budget_s and time.time() - t0 > budget_s:
+            log(f"budget reached after {done} of {len(groups)} shapes")
+            break
+    tmp = db.path.with_suffix(".tmp")
+    tmp.write_text("".join(json.dumps(r) + "\n" for r in db.rows))
+    tmp.replace(db.path)
+    return db, done, len(groups)
+
+
 def main(argv=None):
-    """python -m mgxbench_b200.autotune {sweep,train,evaluate,choose} ...
+    """python -m mgxbench_b200.autotune {sweep,refresh,train,evaluate,choose} ...
 
     sweep     measure the training set and the exhaustive held-out sweep into a JSONL database
+    refresh   measure again the database rows of some tile ids (after a change to their kernels)
     train     fit the MLP on the GPU from the database's training rows and save its weights
     evaluate  regret of the MLP and of the regression baseline against the held-out sweep
     choose    the configuration the saved MLP picks for one problem
@@ -460,6 +497,11 @@ def main(argv=None):
     sw.add_argument("--heldout", type=int, default=500)
     sw.add_argument("--seed", type=int, default=0)
     sw.add_argument("--budget", type=float, default=None, help="stop after this many seconds (resumable)")
+    rf = sub.add_parser("refresh")
+    rf.add_argument("--db", required=True)
+    rf.add_argument("--tiles", required=True, help="comma-separated tile ids, e.g. 0,1,2,3,4,9,10,11,12,13")
+    rf.add_argument("--seed", type=int, default=0)
+    rf.add_argument("--budget", type=float, default=None, help="stop after this many seconds (resumable)")
     tr = sub.add_parser("train")
     tr.add_argument("--db", required=True)
     tr.add_argument("--out", required=True)
@@ -478,6 +520,9 @@ def main(argv=None):
     if a.cmd == "sweep":
         db = run_sweep(a.db, a.train, a.heldout, a.seed, a.budget)
         print(json.dumps({"rows": len(db.rows), "digest": db.digest()}))
+    elif a.cmd == "refresh":
+        db, done, total = refresh_rows(a.db, [int(t) for t in a.tiles.split(",")], a.seed, budget_s=a.budget)
+        print(json.dumps({"rows": len(db.rows), "shapes_refreshed": done, "shapes": total, "digest": db.digest()}))
     elif a.cmd == "train":
         db = SweepDB(a.db)
         rows = [r for r in db.rows if r.get("set") == "train"]

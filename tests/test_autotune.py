@@ -103,3 +103,45 @@ def test_sweep_db_append_and_resume(tmp_path):
     assert len(db2.rows) == 3 and db2.has(256, 512, 1024, 3, at.candidates()[0])
     assert not db2.has(256, 512, 1024, 3, at.candidates()[5])
     assert len(db2.digest()) == 16
+
+
+def test_refresh_rows_measures_again_with_the_sweep_inputs(tmp_path, monkeypatch):
+    """refresh_rows measures again only the rows of the given tile ids, with the seed the sweep
+    used for that shape (train: its index; held-out: 100000 + index), keeps the row order and the
+    set, and skips rows it has already refreshed."""
+    train = [s for s in at.random_shapes(8, 1) if at.shape_fits(*s[:3])][:4]
+    held = [s for s in at.random_shapes(4, 2) if at.shape_fits(*s[:3])][:2]
+    rows = []
+    for i, s in enumerate(train):
+        r = synthetic_rows([s])[i % 3]
+        r["set"] = "train"
+        rows.append(r)
+    for s in held:
+        for r in synthetic_rows([s])[:4]:
+            r["set"] = "heldout"
+            rows.append(r)
+    db = at.SweepDB(tmp_path / "s.jsonl")
+    db.add(rows)
+    tiles = {at.TILE_FP64, at.TILE_FP64_K2}
+    calls = []
+
+    def fake_measure(m, n, k, er, cands, seed=0, **kw):
+        calls.append(((m, n, k, er), tuple(c.tile for c in cands), seed))
+        return [{"m": m, "n": n, "k": k, "exp_range": er, "tile": c.tile, "splits": c.splits, "seconds": 1.0,
+                 "tflops": 1.0, "error": 1e-16} for c in cands]
+
+    monkeypatch.setattr(at, "measure", fake_measure)
+    out, done, total = at.refresh_rows(tmp_path / "s.jsonl", tiles, train_shapes=4, heldout_shapes=2, log=lambda *_: None)
+    again = at.SweepDB(tmp_path / "s.jsonl").rows
+    assert [at.SweepDB.key(r) for r in again] == [at.SweepDB.key(r) for r in rows]
+    assert [r["set"] for r in again] == [r["set"] for r in rows]
+    for old, new in zip(rows, again):
+        assert (new["seconds"] == 1.0) == (old["tile"] in tiles)
+        assert ("refreshed" in new) == (old["tile"] in tiles)
+    seeds = {s: i for i, s in enumerate(train)}
+    seeds.update({s: 100000 + i for i, s in enumerate(held)})
+    assert calls and all(seed == seeds[shape] for shape, _, seed in calls)
+    assert done == total == len(calls)
+    calls.clear()
+    at.refresh_rows(tmp_path / "s.jsonl", tiles, train_shapes=4, heldout_shapes=2, log=lambda *_: None)
+    assert calls == []
