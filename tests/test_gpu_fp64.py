@@ -317,3 +317,40 @@ def test_streamk_beta_one_and_odd_pitch(mgx, oracle):
     ref = C0 + oracle.ab_multiply(np.ascontiguousarray(A), np.ascontiguousarray(B))
     assert np.all(np.abs(host(dC) - ref) <= 2 * gamma(k + 1) * (np.abs(A) @ np.abs(B) + np.abs(C0)))
     assert mgx.device_status() == 0
+
+
+@pytest.mark.parametrize("ksplit,tile_m", [(1, 128), (1, 64), (0, 64), (4, 128)])
+def test_dependent_launches_keep_stream_order(mgx, ksplit, tile_m):
+    """The FP64 kernels are programmatic dependent launches: each one's set-up overlaps the end of
+    the previous kernel in the stream, and it touches memory only after that kernel has finished.
+    Chained products (each reads the previous one's output) and repeated C += A B on one C,
+    issued back to back, give the same bits as the same calls with a full synchronisation
+    between them."""
+    import torch
+    rng = np.random.default_rng(31 + ksplit + tile_m)
+    n = 512
+    A = dev(rng_matrix(rng, (n, n))) / n
+    B = dev(rng_matrix(rng, (n, n))) / n
+
+    def chain(sync):
+        xs = [A]
+        for _ in range(4):
+            y = torch.empty_like(A)
+            mgx.gemm_fp64(xs[-1], B, y, ksplit=ksplit, tile_m=tile_m)
+            if sync:
+                torch.cuda.synchronize()
+            xs.append(y)
+        c = torch.zeros_like(A)
+        for _ in range(4):
+            mgx.gemm_fp64(A, B, c, beta_one=True, ksplit=ksplit, tile_m=tile_m)
+            if sync:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        return xs[1:], c
+
+    ys1, c1 = chain(False)
+    ys2, c2 = chain(True)
+    for a, b in zip(ys1, ys2):
+        assert torch.equal(a.view(torch.int64), b.view(torch.int64))
+    assert torch.equal(c1.view(torch.int64), c2.view(torch.int64))
+    assert mgx.device_status() == 0
