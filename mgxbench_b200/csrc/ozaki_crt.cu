@@ -115,15 +115,30 @@ __device__ __forceinline__ double scale2(double x, int e)
     return __dmul_rn(__dmul_rn(x, pow2i(e1)), pow2i(e2));
 }
 
-// ceil(|x| 2^(22-e))^2 for x != 0 (at least 1), 0 for x == 0.
-__device__ __forceinline__ unsigned long long sq_term(double x, int e)
+// 2^e as f1 f2, the factors scale2 multiplies by (f2 = 1 when one factor is enough).
+__device__ __forceinline__ void scale_factors(int e, double &f1, double &f2)
+{
+    if (e >= -1022 && e <= 1023) {
+        f1 = pow2i(e);
+        f2 = 1.0;
+    } else {
+        const int e1 = e / 2;
+        f1 = pow2i(e1);
+        f2 = pow2i(e - e1);
+    }
+}
+
+// ceil(|x| 2^(22-e))^2 for x != 0 (at least 1), 0 for x == 0, with 2^(22-e) = f1 f2 as
+// scale_factors gives it (the same products as scale2).  |x| < 2^e, so the ceiling is an integer
+// in [1, 2^22]: its low 32 bits come from 2^52 + c, and the square is one 32 x 32 -> 64 multiply.
+__device__ __forceinline__ unsigned long long sq_term(double x, double f1, double f2)
 {
     const double ax = fabs(x);
     if (ax == 0.0) return 0ull;
-    double c = ceil(scale2(ax, 22 - e));
+    double c = ceil(__dmul_rn(__dmul_rn(ax, f1), f2));
     if (c < 1.0) c = 1.0;
-    const unsigned long long ci = (unsigned long long)c;
-    return ci * ci;
+    const uint32_t ci = (uint32_t)__double2loint(__dadd_rn(c, 4503599627370496.0));
+    return (unsigned long long)ci * ci;
 }
 
 // Scale exponent from the exponent of the maximum and the integer sum of squares.
@@ -180,9 +195,20 @@ __global__ void __launch_bounds__(ROW_THREADS) crt_row_scale(const double *__res
         return;
     }
     const int e = frexp_exp_bits(mx);
-    unsigned long long S = 0;
-    if (mx != 0)
-        for (int kk = threadIdx.x; kk < k; kk += ROW_THREADS) S += sq_term(__ldg(r + kk), e);
+    double f1, f2;
+    scale_factors(22 - e, f1, f2);
+    unsigned long long S = 0;  // an exact integer sum: the order of its terms does not matter
+    if (mx != 0) {
+        int kk = threadIdx.x;
+        for (; kk + 3 * ROW_THREADS < k; kk += 4 * ROW_THREADS) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = __ldg(r + kk + u * ROW_THREADS);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) S += sq_term(v[u], f1, f2);
+        }
+        for (; kk < k; kk += ROW_THREADS) S += sq_term(__ldg(r + kk), f1, f2);
+    }
     for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
     if (lane == 0) red[warp] = S;   // warp 0 read red[] before the barrier above
     __syncthreads();
@@ -218,11 +244,21 @@ __global__ void crt_col_sumsq(const double *__restrict__ B, int k, int n, int ld
     const unsigned long long mx = colmax[j];
     if (mx == 0 || mx >= 0x7ff0000000000000ull) return;
     const int e = frexp_exp_bits(mx);
+    double f1, f2;
+    scale_factors(22 - e, f1, f2);
     const int rows_per = (k + gridDim.y - 1) / gridDim.y;
     const int r0 = blockIdx.y * rows_per;
     const int r1 = min(k, r0 + rows_per);
-    unsigned long long S = 0;
-    for (int r = r0; r < r1; ++r) S += sq_term(__ldg(B + (size_t)r * ldb + j), e);
+    unsigned long long S = 0;  // an exact integer sum: the order of its terms does not matter
+    int r = r0;
+    for (; r + 8 <= r1; r += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldg(B + (size_t)(r + u) * ldb + j);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) S += sq_term(v[u], f1, f2);
+    }
+    for (; r < r1; ++r) S += sq_term(__ldg(B + (size_t)r * ldb + j), f1, f2);
     if (S) atomicAdd(colsum + j, S);
 }
 
@@ -254,19 +290,6 @@ __global__ void crt_col_scale(const unsigned long long *__restrict__ colmax, con
 // (residue_word): a modulus's constants are read once per 8 values, and the 8 residue bytes
 // pack into two words with byte permutes.
 constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
-
-// 2^e as f1 f2, the factors scale2 multiplies by (f2 = 1 when one factor is enough).
-__device__ __forceinline__ void scale_factors(int e, double &f1, double &f2)
-{
-    if (e >= -1022 && e <= 1023) {
-        f1 = pow2i(e);
-        f2 = 1.0;
-    } else {
-        const int e1 = e / 2;
-        f1 = pow2i(e1);
-        f2 = pow2i(e - e1);
-    }
-}
 
 // x = rint(v 2^sg) as xh 2^32 + xl; returns xh and xl + 1.5 * 2^52.
 __device__ __forceinline__ void split32(double v, double f1, double f2, double &xh, double &xr)
